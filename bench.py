@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the Biot/CPML stepper (one JSON line on stdout).
+
+Workload: the 2D x-z layered model of 4000 x 2000 cells (+ a 20-cell CPML on
+every face: 4040 x 2040 padded, 8.22 M updated cells per step), dx 5 m,
+dt 0.4 ms, 25 Hz Ricker at (2000, 10) on txx/tzz and p, 2000 receivers at
+depth 10, second-order stencil, seeded synthetic layers (seed 1).  A "step"
+is one time step over the whole grid (velocity phase, stress phase, trace
+recording and source injection).  The inputs (1.0 GB FP32 state + coefficients)
+are larger than the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours:       FP32 path (the headline `value`), COMP16 path and an FP64 run of
+            the same steps for the seismogram relative L2 of both, device
+            timed with CUDA events on the library's stream; `e2e` through the
+            public API with pinned host buffers; `roofline` of the dominant
+            kernel; `cpu_baseline` = the oracle (C++/OpenMP restatement of the
+            reference arithmetic) on a bounded sample, on rank 0 at N = 1.
+reference:  the reference's arithmetic on the host cores (the oracle, all
+            threads), same workload and metric.  The reference itself is a
+            CUDA program with no CPU implementation.
+N > 1 runs independent replicas (one shot per GPU, no collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mcell-updates/s"
+WORKLOAD = "c1: 2D x-z layered 4000x2000 (+20-cell CPML), order 2, dt 0.4 ms, 25 Hz, 2000 receivers"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nx", type=int, default=4000)
+    ap.add_argument("--nz", type=int, default=2000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=20)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def workload(precision, nt, nx, nz):
+    from mixedprecisionfaracoustic_b200.presets import config1
+    return config1(precision=precision, seed=1, nx=nx, nz=nz, nt=nt)
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the dominant kernels from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return {}
+    return {}
+
+
+def run_ours(args, rank, ws):
+    import torch
+    from mixedprecisionfaracoustic_b200 import Simulation
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    K, W, P = args.steps, args.warmup, args.profile_steps
+    nt = W + K + P
+    peak, peak_kind = measured_peaks()
+    res = {}
+    sims = {}
+    for prec in ("fp32", "comp16"):
+        cfg, med = workload(prec, nt, args.nx, args.nz)
+        cfg.device = dev
+        s = Simulation(cfg, med)
+        s.run(W)
+        s.sync()
+        if ws > 1:
+            torch.distributed.barrier()
+        l0 = s.launch_count()
+        with ClockSampler(dev) as clk:
+            ms = s.run_timed(K)
+        launches = s.launch_count() - l0
+        if ws > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        (bv, bt), cells = s.algorithmic_bytes()
+        pv, pt, pp = s.profile_phases(P)
+        dom = "v_phase" if pv >= pt else "t_phase"
+        t_dom = max(pv, pt)
+        b_dom = (bv if pv >= pt else bt) * cells
+        achieved = b_dom / (t_dom * 1e-3) / 1e9
+        res[prec] = {
+            "value": cells * K * ws / (ms * 1e-3) / 1e6,
+            "ms_per_step": ms / K,
+            "launches": launches,
+            "clocks": clk.summary(),
+            "phase_ms": {"v_phase": pv, "t_phase": pt, "record_inject": pp},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "bytes_per_cell": {"v_phase": bv, "t_phase": bt},
+                         "step_frac": (bv + bt) * cells / ((pv + pt) * 1e-3) / 1e9 / peak},
+            "cells": cells,
+        }
+        sims[prec] = s
+    # FP64 run of the same steps: seismogram relative L2 of both paths
+    cfg, med = workload("fp64", nt, args.nx, args.nz)
+    cfg.device = dev
+    s64 = Simulation(cfg, med)
+    s64.run(W + K + P)
+    s64.sync()
+    for prec in ("fp32", "comp16"):
+        res[prec]["rel_l2_vs_fp64"] = {c: sims[prec].trace_rel_l2(s64, c) for c in ("txx", "tzz", "vux", "p")}
+    s64.close()
+    for s in sims.values():
+        s.close()
+    # end to end through the public API: pinned host medium in, traces out
+    cfg, med = workload("fp32", K, args.nx, args.nz)
+    cfg.device = dev
+    pinned = {}
+    for k, v in med.items():
+        t = torch.empty(v.shape, dtype=torch.float32, pin_memory=True)
+        t.numpy()[...] = v
+        pinned[k] = t.numpy()
+    from mixedprecisionfaracoustic_b200.biot import Medium
+    pm = Medium(pinned)
+    h2d = sum(a.nbytes for a in pinned.values())
+    if ws > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    s = Simulation(cfg, pm)
+    s.run(K)
+    tr = [s.traces(c) for c in ("txx", "tzz", "vux", "vwx", "p")]
+    e2e_s = time.perf_counter() - t0
+    s.close()
+    d2h = sum(a.nbytes for a in tr)
+    if ws > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": res["fp32"]["cells"] * K * ws / e2e_s / 1e6, "unit": METRIC,
+           "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K, "seconds": e2e_s,
+           "path": "bp_create(pinned host medium) + bp_run(K) + bp_get_traces x5 + bp_destroy"}
+    return res, e2e
+
+
+def cpu_baseline(args, budget_s=20.0):
+    """The oracle (REF32, all host threads) on a bounded sample of the workload."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    nz = args.nz
+    cfg, med = workload("fp32", 64, args.nx, nz)
+    o = O.Oracle(cfg, med, O.REF32)
+    o.run(1)
+    t0 = time.perf_counter()
+    o.run(2)
+    per = (time.perf_counter() - t0) / 2
+    n = int(max(2, min(60, budget_s / max(per, 1e-6))))
+    n = min(n, cfg.nt - 3)
+    t0 = time.perf_counter()
+    o.run(n)
+    el = time.perf_counter() - t0
+    cells = (cfg.padded[0] - 2) * (cfg.padded[2] - 2)
+    o.close()
+    return {"value": cells * n / el / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"c1 full {cfg.padded[0]}x{cfg.padded[2]} grid, steps 3..{3 + n} ({el:.1f} s), REF32 arithmetic"}
+
+
+def run_reference(args, rank, ws):
+    """Reference arm: the reference's update equations on the host cores."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    K, W = args.steps, args.warmup
+    nz = args.nz
+    cfg, med = workload("fp32", 4, args.nx, nz)
+    probe = O.Oracle(cfg, med, O.REF32)
+    probe.run(1)
+    t0 = time.perf_counter()
+    probe.run(1)
+    per_full = time.perf_counter() - t0
+    probe.close()
+    budget = 150.0
+    if (K + W) * per_full > budget:      # bounded sample: fewer rows, same nx and medium statistics
+        nz = max(64, int(nz * budget / ((K + W) * per_full)))
+    cfg, med = workload("fp32", K + W + 1, args.nx, nz)
+    o = O.Oracle(cfg, med, O.REF32)
+    o.run(W)
+    t0 = time.perf_counter()
+    o.run(K)
+    el = time.perf_counter() - t0
+    cells = (cfg.padded[0] - 2) * (cfg.padded[2] - 2)
+    v = cells * K / el / 1e6
+    sample = f"{cfg.padded[0]}x{cfg.padded[2]} grid ({nz} of {args.nz} physical rows), {K} steps, REF32"
+    return {"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus, "steps": K, "warmup": W,
+            "ms_per_step": el / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "global_batch": 1, "seq_len": None, "parallelism": "replicas"},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        if args.impl == "reference":
+            if rank != 0:
+                return 0
+        else:
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    if args.impl == "reference":
+        print(json.dumps(run_reference(args, rank, ws)), flush=True)
+        return 0
+    res, e2e = run_ours(args, rank, ws)
+    out = None
+    if rank == 0:
+        f32, c16 = res["fp32"], res["comp16"]
+        cpu = None if (args.no_cpu_baseline or ws > 1) else cpu_baseline(args)
+        traffic = ncu_traffic()
+        roof = dict(f32["roofline"])
+        tk = traffic.get(f"fp32_{roof['kernel']}")
+        roof["traffic"] = tk
+        c16roof = dict(c16["roofline"])
+        c16roof["traffic"] = traffic.get(f"comp16_{c16roof['kernel']}")
+        out = {
+            "metric": METRIC, "value": f32["value"], "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": f32["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": [args.nx + 40, args.nz + 40], "order": 2,
+                       "global_batch": ws, "seq_len": None, "parallelism": f"replicas x{ws}",
+                       "l2_flush": "inputs larger than L2 (1.0 GB working set)"},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": f32["launches"],
+            "clocks": f32["clocks"],
+            "rel_l2_vs_fp64": f32["rel_l2_vs_fp64"],
+            "phase_ms": f32["phase_ms"],
+            "comp16": {"value": c16["value"], "ms_per_step": c16["ms_per_step"], "roofline": c16roof,
+                       "rel_l2_vs_fp64": c16["rel_l2_vs_fp64"], "phase_ms": c16["phase_ms"],
+                       "gpu_launches": c16["launches"], "clocks": c16["clocks"],
+                       "speedup_vs_fp32": c16["value"] / f32["value"]},
+        }
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

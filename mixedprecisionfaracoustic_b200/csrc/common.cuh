@@ -1,0 +1,209 @@
+// common.cuh - device-side data layout, precision policies and helpers shared
+// by the precompute, step and reduction kernels.
+//
+// HBM layout of one shot ("padded" grid nx x ny x nz, ny = 1 in 2D):
+//   * every field / coefficient is a separate array, x fastest, with a row
+//     pitch rounded up to 32 elements so 4-cell chunks are 16-byte aligned
+//     (FP32) and every row starts on a 128-byte boundary;
+//     index(x, y, z) = x + y * pitch + z * pitch * ny.
+//   * CPML memory variables (ψ and the previous derivative, 2 per derivative
+//     slot) exist only on the absorbing slabs of their axis (the reference
+//     keeps 48 full-volume arrays, Float/main.cu:707-755).
+//   * COMP16 fields are two arrays: fp16 "hi" and int8 residual "lo".
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/biot.h"
+
+namespace bpk {
+
+// V-phase coefficient slots (FP32/FP64: reference-shaped; COMP16: scaled set)
+//  FP32/FP64: RHO_X,Y,Z = rho^-1 on faces (Float/main.cu:499-501), RHOF cell,
+//             CC1_X..Z, CC2_X..Z = C2 - rhof^2 rho^-1 +/- C1 DT/2 (:106-113),
+//             CC1 = 0 marks a face with C1 == 0 (vw forced to 0, :160-185).
+//  COMP16:    RHO_* = 2^-em DT rho^-1, RHOF = rhof 2^em / DT, CC1_* = Aw,
+//             CC2_* = Bp (Half/main.cu:986-1012); Bt = rhof rho^-1 Bp in-kernel.
+enum VCoef { VC_RHO_X, VC_RHO_Y, VC_RHO_Z, VC_RHOF, VC_CC1_X, VC_CC1_Y, VC_CC1_Z,
+             VC_CC2_X, VC_CC2_Y, VC_CC2_Z, VC_COUNT };
+// T-phase coefficients: C, M, H, H-2mu at the cell; harmonic mu on edges
+// (Float/main.cu:480-491).  COMP16 stores 2^em DT times each (Half :1023-1029).
+enum TCoef { TC_C, TC_M, TC_H, TC_H2U, TC_MUXY, TC_MUXZ, TC_MUYZ, TC_COUNT };
+
+// CPML slab of one axis: cells [0, lo) and [hi0, n) carry memory variables.
+struct Slab {
+    int lo;      // cells [0, lo)
+    int hi0;     // cells [hi0, n)
+    int width;   // lo + (n - hi0), x axis rounded up to a multiple of 4
+    __host__ __device__ int index(int i) const {
+        return i < lo ? i : (i >= hi0 ? lo + (i - hi0) : -1);
+    }
+};
+
+struct ShotDesc {
+    int dim, order, hw;           // hw = order / 2 = untouched border cells
+    int nx, ny, nz;               // padded extents
+    int pitch;                    // row pitch (elements)
+    long long plane;              // pitch * ny
+    int nseg;                     // 128-cell x segments per row
+    int nrows;                    // rows per shot: ny * nz (3D) or nz (2D)
+    long long tile0;              // first tile index of this shot in the batch
+    int rows_per_tile;
+    int nt;                       // trace length
+    int src_idx_valid;
+    long long src_idx;            // flat index of the source cell
+    int src_mask;
+    int nrec;
+    const long long* rec_idx;     // flat indices
+    float* traces;                // [BP_NTRACE][nrec][nt]
+    double* traces64;             // FP64 runs: [BP_NTRACE][nrec][nt]
+    const void* wavelet;          // source samples per step (float or double)
+    const float* dyn;             // COMP16: state scale during step it (nt entries)
+    float out_stress, out_vel;    // COMP16: 2^-es, 2^(em-es) (divided by dyn at use)
+    float inj_scale;              // COMP16: 2^es
+    float dt;                     // DT (FP32/COMP16)
+    double dtd;                   // DT (FP64)
+    float inv_h;                  // 1/H (COMP16 multiplies; FP32/FP64 divide by H like the reference)
+    float h;                      // H
+    double hd;
+    void* f[BP_NFIELDS];          // field arrays (hi for COMP16)
+    int8_t* flo[BP_NFIELDS];      // COMP16 residuals
+    void* vc[VC_COUNT];
+    int8_t* vclo[VC_COUNT];
+    void* tc[TC_COUNT];
+    int8_t* tclo[TC_COUNT];
+    // CPML: per axis tables of length n (b = -DT d / 2, e = exp(-d DT)) on the
+    // integer (b, e) and half (b2, e2) grids, and the slab memory variables.
+    const void* pb[3];
+    const void* pe[3];
+    const void* pb2[3];
+    const void* pe2[3];
+    Slab slab[3];
+    void* psiV[3];                // per axis: [2*nslot][slab cells] (ψ then prev)
+    void* psiT[3];
+    long long slab_cells[3];
+    int done;                     // batch: slot empty or retired, skip its tiles
+    int* step_base;               // device: step index `it` of step k=0 of the current chunk
+    const float* rtab;            // COMP16: per-step factor applied to old state (dyn[it]/dyn[it-1])
+    int src_rec;                  // receiver index that owns the source cell, or -1
+    template <class R>
+    __device__ __forceinline__ R dtr() const { return sizeof(R) == 8 ? (R)dtd : (R)dt; }
+};
+
+// Steps are issued in chunks; step k of a chunk of shot s has index
+// it = *step_base + k.  Reading the base from device memory lets one captured
+// CUDA graph serve every chunk: k_advance moves the bases after each chunk.
+
+// ---------------------------------------------------------------------------
+// Compensated FP16 codec (the reference's store_ch / load_ch,
+// Half/main.cu:59-100): value ~ hi + lo * u(hi), u = fp16 ulp(hi) / 256
+// = 2^(e-19) with e the frexp exponent of |hi|, and u = 2^-32 for |hi| < 2^-14.
+// The exponent is taken from the fp32 bit pattern (exact, same as frexpf).
+__device__ __forceinline__ float residual_unit(float hi) {
+    float a = fabsf(hi);
+    if (a < 6.103515625e-5f) return 2.3283064365386963e-10f;
+    unsigned u = __float_as_uint(a);
+    int e = (int)((u >> 23) & 0xff) - 126;   // frexpf exponent: a = m * 2^e, m in [0.5,1)
+    return __uint_as_float((unsigned)(e - 19 + 127) << 23);
+}
+__device__ __forceinline__ float decode_ch(__half hi, int8_t lo) {
+    float h = __half2float(hi);
+    return h + (float)lo * residual_unit(h);
+}
+__device__ __forceinline__ void encode_ch(float v, __half& hi, int8_t& lo) {
+    __half h = __float2half_rn(v);
+    float hf = __half2float(h);
+    float scaled = (v - hf) / residual_unit(hf);
+    int q = (int)(scaled + (scaled >= 0.0f ? 0.5f : -0.5f));
+    q = q > 127 ? 127 : (q < -127 ? -127 : q);
+    hi = h;
+    lo = (int8_t)q;
+}
+
+// ---------------------------------------------------------------------------
+// Precision policies: storage of fields/coefficients and the arithmetic type.
+struct PolF32 {
+    using real = float;
+    static constexpr int prec = BP_PREC_FP32;
+    __device__ __forceinline__ static void ld4(const void* p, const int8_t*, long long i, real (&v)[4]) {
+        float4 t = *reinterpret_cast<const float4*>(static_cast<const float*>(p) + i);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
+    __device__ __forceinline__ static real ld1(const void* p, const int8_t*, long long i) {
+        return static_cast<const float*>(p)[i];
+    }
+    __device__ __forceinline__ static void st4(void* p, int8_t*, long long i, const real (&v)[4]) {
+        *reinterpret_cast<float4*>(static_cast<float*>(p) + i) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+    __device__ __forceinline__ static void st1(void* p, int8_t*, long long i, real v) {
+        static_cast<float*>(p)[i] = v;
+    }
+};
+
+struct PolF64 {
+    using real = double;
+    static constexpr int prec = BP_PREC_FP64;
+    __device__ __forceinline__ static void ld4(const void* p, const int8_t*, long long i, real (&v)[4]) {
+        const double2* q = reinterpret_cast<const double2*>(static_cast<const double*>(p) + i);
+        double2 a = q[0], b = q[1];
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    }
+    __device__ __forceinline__ static real ld1(const void* p, const int8_t*, long long i) {
+        return static_cast<const double*>(p)[i];
+    }
+    __device__ __forceinline__ static void st4(void* p, int8_t*, long long i, const real (&v)[4]) {
+        double2* q = reinterpret_cast<double2*>(static_cast<double*>(p) + i);
+        q[0] = make_double2(v[0], v[1]);
+        q[1] = make_double2(v[2], v[3]);
+    }
+    __device__ __forceinline__ static void st1(void* p, int8_t*, long long i, real v) {
+        static_cast<double*>(p)[i] = v;
+    }
+};
+
+// COMP16: fp16 hi (8 bytes per 4 cells) + int8 lo (4 bytes per 4 cells).
+// A null lo pointer means "hi only" (used for fp16-only coefficient storage).
+struct PolC16 {
+    using real = float;
+    static constexpr int prec = BP_PREC_COMP16;
+    __device__ __forceinline__ static void ld4(const void* p, const int8_t* lo, long long i, real (&v)[4]) {
+        uint2 h = *reinterpret_cast<const uint2*>(static_cast<const __half*>(p) + i);
+        __half2 h01 = *reinterpret_cast<__half2*>(&h.x);
+        __half2 h23 = *reinterpret_cast<__half2*>(&h.y);
+        __half hs[4] = {__low2half(h01), __high2half(h01), __low2half(h23), __high2half(h23)};
+        if (lo) {
+            char4 l = *reinterpret_cast<const char4*>(lo + i);
+            v[0] = decode_ch(hs[0], l.x); v[1] = decode_ch(hs[1], l.y);
+            v[2] = decode_ch(hs[2], l.z); v[3] = decode_ch(hs[3], l.w);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) v[j] = __half2float(hs[j]);
+        }
+    }
+    __device__ __forceinline__ static real ld1(const void* p, const int8_t* lo, long long i) {
+        __half h = static_cast<const __half*>(p)[i];
+        return lo ? decode_ch(h, lo[i]) : __half2float(h);
+    }
+    __device__ __forceinline__ static void st4(void* p, int8_t* lo, long long i, const real (&v)[4]) {
+        __half hs[4];
+        int8_t ls[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) encode_ch(v[j], hs[j], ls[j]);
+        uint2 h;
+        __half2 a = __halves2half2(hs[0], hs[1]), b = __halves2half2(hs[2], hs[3]);
+        h.x = *reinterpret_cast<unsigned*>(&a);
+        h.y = *reinterpret_cast<unsigned*>(&b);
+        *reinterpret_cast<uint2*>(static_cast<__half*>(p) + i) = h;
+        *reinterpret_cast<char4*>(lo + i) = make_char4(ls[0], ls[1], ls[2], ls[3]);
+    }
+    __device__ __forceinline__ static void st1(void* p, int8_t* lo, long long i, real v) {
+        __half h;
+        int8_t l;
+        encode_ch(v, h, l);
+        static_cast<__half*>(p)[i] = h;
+        lo[i] = l;
+    }
+};
+
+}  // namespace bpk

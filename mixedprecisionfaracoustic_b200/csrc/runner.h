@@ -1,0 +1,85 @@
+// runner.h - issues chunks of time steps for a set of shot descriptors, either
+// as direct launches or by replaying a captured CUDA graph of S steps.
+#pragma once
+#include "shot.h"
+
+namespace bpk {
+
+struct Runner {
+    int prec = 0, dim = 2, order = 2;
+    const ShotDesc* d_shots = nullptr;
+    int nshots = 0;
+    long long ntiles = 0;
+    int max_rec = 0;
+    int grid_v = 1, grid_t = 1;
+    cudaStream_t st = nullptr;
+    int graph_steps = 0;               // S; 0 disables graphs
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool graph_failed = false;
+    long long launches = 0;            // kernels issued (graph replays count their nodes)
+
+    void configure(int prec_, int dim_, int order_, const ShotDesc* d, int n, long long tiles, int maxrec,
+                   cudaStream_t s, int ctas_per_sm, int steps_per_graph) {
+        prec = prec_; dim = dim_; order = order_;
+        d_shots = d; nshots = n; ntiles = tiles; max_rec = maxrec; st = s;
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int ov = phase_occupancy(prec, dim, order, true), ot = phase_occupancy(prec, dim, order, false);
+        if (ctas_per_sm > 0) { ov = ov < ctas_per_sm ? ov : ctas_per_sm; ot = ot < ctas_per_sm ? ot : ctas_per_sm; }
+        long long gv = (long long)ov * sms, gt = (long long)ot * sms;
+        grid_v = (int)(gv < tiles ? gv : (tiles > 0 ? tiles : 1));
+        grid_t = (int)(gt < tiles ? gt : (tiles > 0 ? tiles : 1));
+        graph_steps = steps_per_graph;
+        reset_graph();
+    }
+    void reset_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        graph_failed = false;
+    }
+    ~Runner() { reset_graph(); }
+
+    // m steps issued directly (k = 0..m-1), then the step bases advance by m.
+    cudaError_t issue(int m, bool count = true) {
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k < m && e == cudaSuccess; k++) {
+            e = launch_phase(prec, dim, order, true, d_shots, nshots, ntiles, k, grid_v, st);
+            if (e == cudaSuccess) e = launch_phase(prec, dim, order, false, d_shots, nshots, ntiles, k, grid_t, st);
+            if (e == cudaSuccess) e = launch_post(prec, d_shots, nshots, max_rec, k, 1, st);
+        }
+        if (e == cudaSuccess) e = launch_advance(d_shots, nshots, m, st);
+        if (count) launches += 3LL * m + 1;
+        return e;
+    }
+    cudaError_t ensure_graph() {
+        if (exec || graph_failed || graph_steps <= 0) return cudaSuccess;
+        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) { graph_failed = true; cudaGetLastError(); return cudaSuccess; }
+        cudaError_t ei = issue(graph_steps, false);
+        e = cudaStreamEndCapture(st, &graph);
+        if (ei != cudaSuccess || e != cudaSuccess) { graph_failed = true; cudaGetLastError(); graph = nullptr; return cudaSuccess; }
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e != cudaSuccess) { graph_failed = true; exec = nullptr; cudaGetLastError(); }
+        return cudaSuccess;
+    }
+    // Runs m steps: full graph replays of S steps, the remainder directly.
+    cudaError_t run(int m) {
+        cudaError_t e = cudaSuccess;
+        if (graph_steps > 0 && m >= graph_steps) {
+            ensure_graph();
+            while (exec && m >= graph_steps && e == cudaSuccess) {
+                e = cudaGraphLaunch(exec, st);
+                launches += 3LL * graph_steps + 1;
+                m -= graph_steps;
+            }
+        }
+        if (m > 0 && e == cudaSuccess) e = issue(m);
+        return e;
+    }
+};
+
+}  // namespace bpk

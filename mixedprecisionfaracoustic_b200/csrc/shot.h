@@ -1,0 +1,74 @@
+// shot.h - host-side owner of one shot's device state (used by the single-shot
+// bp_sim, the batch and the server).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace bpk {
+
+// launchers (step.cu, precompute.cu, reduce.cu)
+cudaError_t launch_phase(int prec, int dim, int order, bool vphase, const ShotDesc* d_shots, int nshots,
+                         long long ntiles, int k, int grid, cudaStream_t st);
+cudaError_t launch_post(int prec, const ShotDesc* d_shots, int nshots, int max_rec, int k, int do_record,
+                        cudaStream_t st);
+cudaError_t launch_inject(int prec, const ShotDesc* d_shots, int nshots, int k, cudaStream_t st);
+cudaError_t launch_advance(const ShotDesc* d_shots, int nshots, int n, cudaStream_t st);
+cudaError_t launch_snapshot(int prec, const ShotDesc* d_shots, int shot, int f, int slice_y, float* out, int it,
+                            cudaStream_t st);
+cudaError_t launch_field_f64(int prec, const ShotDesc* d_shots, int f, double* out, cudaStream_t st);
+cudaError_t launch_coef(int prec, const ShotDesc* d_shots, int which, float* out, cudaStream_t st);
+int phase_threads();
+int tile_rows();
+int seg_cells();
+int phase_occupancy(int prec, int dim, int order, bool vphase);
+
+void host_pml_region(int n, int np, float H, int i, bool* left, bool* right);
+cudaError_t launch_profile(int prec, int n, int np, float H, double dt, double v0, double rc, void* b, void* e,
+                           void* b2, void* e2, cudaStream_t st);
+cudaError_t launch_coefs(int prec, const ShotDesc& S, const float* const* med, int pnx, int pny, int pnz, int np,
+                         double dt, int em, cudaStream_t st);
+int scan_kr_blocks();
+cudaError_t launch_scan_kr(int dim, int nx, int ny, int nz, const float* const* med, int pnx, int pny, int pnz,
+                           int np, double* partial, double* out, cudaStream_t st);
+int reduce_blocks();
+cudaError_t launch_energy(int prec, const ShotDesc* d_shots, double* partial, double* out, cudaStream_t st);
+cudaError_t launch_rel_l2(const float* x, const float* ref, long long n, double* partial, double* out,
+                          cudaStream_t st);
+
+void set_error(const std::string& msg);
+
+struct Shot {
+    bp_config cfg{};
+    std::vector<int> rec_x, rec_y, rec_z, snap_steps;
+    std::vector<unsigned> snap_masks;
+    std::vector<int> urec_of;          // receiver -> unique receiver cell
+    int nurec = 0;
+    ShotDesc desc{};                   // host copy of the device descriptor
+    ShotDesc* d_desc = nullptr;        // device copy (single-shot runs)
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    int em = 0, es = 0;
+    double kmax = 0, rmax = 0;
+    std::vector<float> dyn;            // COMP16 state scale per step
+    float* d_snap = nullptr;
+    size_t snap_n = 0;                 // floats per snapshot field
+    std::vector<long long> snap_off;   // [k * 13 + f] offset in d_snap, -1 if not captured
+    double* d_scratch = nullptr;       // reductions
+    double* d_out = nullptr;           // 4 doubles
+    long long cells = 0;               // updated cells per step
+    int it_host = 0;                   // steps issued so far
+    long long ntiles = 0;
+
+    // Computes the arena size for cfg without allocating (admission control).
+    static int plan_bytes(const bp_config* cfg, size_t* bytes);
+    int create(const bp_config* cfg, const bp_medium* med, cudaStream_t st);
+    void destroy();
+};
+
+int validate_config(const bp_config* cfg);
+
+}  // namespace bpk

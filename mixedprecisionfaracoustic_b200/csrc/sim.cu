@@ -1,0 +1,432 @@
+// sim.cu - the single-shot C ABI (bp_sim) and the reference-format writers.
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "runner.h"
+
+namespace bpk {
+const char* last_error_cstr();
+}
+using namespace bpk;
+
+struct bp_sim {
+    Shot shot;
+    Runner run;
+    cudaStream_t st = nullptr;
+    int device = 0;
+};
+
+#define SIM_CK(call)                                                                       \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+            return e_ == cudaErrorMemoryAllocation ? BP_ERR_OOM : BP_ERR_CUDA;             \
+        }                                                                                  \
+    } while (0)
+
+static const char* kFieldNames[BP_NFIELDS] = {"vux", "vuy", "vuz", "vwx", "vwy", "vwz", "p",
+                                              "txx", "tyy", "tzz", "txy", "txz", "tyz"};
+
+static int check_device(int device) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        set_error(std::string("no CUDA device: ") + cudaGetErrorString(e));
+        return BP_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) { set_error("device ordinal out of range"); return BP_ERR_ARG; }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { set_error("cudaGetDeviceProperties failed"); return BP_ERR_NO_DEVICE; }
+    if (prop.major != 10) {
+        set_error("this library is built for sm_100a (B200); device is sm_" + std::to_string(prop.major) + std::to_string(prop.minor));
+        return BP_ERR_NO_DEVICE;
+    }
+    return BP_OK;
+}
+
+extern "C" {
+
+const char* bp_error_string(int code) {
+    switch (code) {
+        case BP_OK: return "ok";
+        case BP_ERR_ARG: return "invalid argument";
+        case BP_ERR_OOM: return "out of memory";
+        case BP_ERR_CUDA: return "CUDA error";
+        case BP_ERR_CFL: return "time step violates the stability limit";
+        case BP_ERR_UNSTABLE: return "non-finite wavefield";
+        case BP_ERR_TIMEOUT: return "timed out";
+        case BP_ERR_STATE: return "invalid state";
+        case BP_ERR_NOT_FOUND: return "not found";
+        case BP_ERR_NO_DEVICE: return "no usable CUDA device";
+        case BP_ERR_BUDGET: return "request exceeds the HBM budget";
+        default: return "unknown error";
+    }
+}
+const char* bp_last_error(void) { return last_error_cstr(); }
+
+int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out) {
+    if (!out) { set_error("null output pointer"); return BP_ERR_ARG; }
+    *out = nullptr;
+    int rc = validate_config(cfg);
+    if (rc) return rc;
+    rc = check_device(cfg->device);
+    if (rc) return rc;
+    if (cfg->check_cfl && medium) {
+        double dtmax = 0, vmax = 0;
+        rc = bp_cfl_limit(cfg, medium, &dtmax, &vmax);
+        if (rc) return rc;
+        if ((double)cfg->dt > dtmax) {
+            char buf[160];
+            snprintf(buf, sizeof buf, "dt=%g exceeds the stability limit %g (vmax=%g m/s)", (double)cfg->dt, dtmax, vmax);
+            set_error(buf);
+            return BP_ERR_CFL;
+        }
+    }
+    SIM_CK(cudaSetDevice(cfg->device));
+    bp_sim* s = new bp_sim();
+    s->device = cfg->device;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); delete s; return BP_ERR_CUDA; }
+    rc = s->shot.create(cfg, medium, s->st);
+    if (rc) { s->shot.destroy(); cudaStreamDestroy(s->st); delete s; return rc; }
+    s->run.configure(cfg->precision, cfg->dim, cfg->order, s->shot.d_desc, 1, s->shot.ntiles, s->shot.nurec, s->st,
+                     0, 32);
+    *out = s;
+    return BP_OK;
+}
+
+int bp_run(bp_sim* s, int nsteps) {
+    if (!s || nsteps < 0) { set_error("bad arguments"); return BP_ERR_ARG; }
+    SIM_CK(cudaSetDevice(s->device));
+    Shot& sh = s->shot;
+    while (nsteps > 0 && sh.it_host < sh.cfg.nt) {
+        int m = std::min(nsteps, sh.cfg.nt - sh.it_host);
+        int next_snap = -1;
+        for (int st : sh.snap_steps)
+            if (st >= sh.it_host && (next_snap < 0 || st < next_snap)) next_snap = st;
+        if (next_snap >= 0) m = std::min(m, next_snap - sh.it_host + 1);
+        SIM_CK(s->run.run(m));
+        sh.it_host += m;
+        const int done_it = sh.it_host - 1;
+        for (int k = 0; k < (int)sh.snap_steps.size(); k++) {
+            if (sh.snap_steps[k] != done_it) continue;
+            for (int f = 0; f < BP_NFIELDS; f++) {
+                long long off = sh.snap_off[(size_t)k * BP_NFIELDS + f];
+                if (off < 0) continue;
+                int sy = (sh.cfg.dim == 3 && sh.cfg.snap_y >= 0) ? sh.cfg.snap_y : -1;
+                SIM_CK(launch_snapshot(sh.cfg.precision, sh.d_desc, 0, f, sy, sh.d_snap + off, done_it, s->st));
+            }
+        }
+        nsteps -= m;
+    }
+    return BP_OK;
+}
+
+int bp_run_timed(bp_sim* s, int nsteps, float* ms) {
+    if (!s || !ms) { set_error("bad arguments"); return BP_ERR_ARG; }
+    SIM_CK(cudaSetDevice(s->device));
+    cudaEvent_t a, b;
+    SIM_CK(cudaEventCreate(&a));
+    SIM_CK(cudaEventCreate(&b));
+    cudaEventRecord(a, s->st);
+    int rc = bp_run(s, nsteps);
+    cudaEventRecord(b, s->st);
+    cudaError_t e = cudaEventSynchronize(b);
+    float t = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
+    *ms = t;
+    return BP_OK;
+}
+
+int bp_sync(bp_sim* s) {
+    if (!s) { set_error("null sim"); return BP_ERR_ARG; }
+    SIM_CK(cudaStreamSynchronize(s->st));
+    return BP_OK;
+}
+
+int bp_get_step(bp_sim* s, int* it) {
+    if (!s || !it) { set_error("bad arguments"); return BP_ERR_ARG; }
+    *it = s->shot.it_host;
+    return BP_OK;
+}
+
+int bp_get_traces(bp_sim* s, int comp, float* host, size_t n) {
+    if (!s || !host || comp < 0 || comp >= BP_NTRACE) { set_error("bad arguments"); return BP_ERR_ARG; }
+    Shot& sh = s->shot;
+    const size_t nt = sh.cfg.nt, nr = sh.cfg.nrec;
+    if (n < nr * nt) { set_error("host buffer too small"); return BP_ERR_ARG; }
+    SIM_CK(cudaStreamSynchronize(s->st));
+    std::vector<float> u((size_t)sh.nurec * nt);
+    if (!u.empty())
+        SIM_CK(cudaMemcpy(u.data(), sh.desc.traces + (size_t)comp * sh.nurec * nt, u.size() * 4, cudaMemcpyDeviceToHost));
+    for (size_t r = 0; r < nr; r++) std::memcpy(host + r * nt, u.data() + (size_t)sh.urec_of[r] * nt, nt * 4);
+    return BP_OK;
+}
+
+int bp_snapshot_size(bp_sim* s, size_t* n) {
+    if (!s || !n) { set_error("bad arguments"); return BP_ERR_ARG; }
+    *n = s->shot.snap_n;
+    return BP_OK;
+}
+
+int bp_get_snapshot(bp_sim* s, int k, int field, float* host, size_t n) {
+    if (!s || !host || field < 0 || field >= BP_NFIELDS) { set_error("bad arguments"); return BP_ERR_ARG; }
+    Shot& sh = s->shot;
+    if (k < 0 || k >= (int)sh.snap_steps.size()) { set_error("no such snapshot"); return BP_ERR_NOT_FOUND; }
+    long long off = sh.snap_off[(size_t)k * BP_NFIELDS + field];
+    if (off < 0) { set_error("field not captured at this snapshot"); return BP_ERR_NOT_FOUND; }
+    if (sh.it_host <= sh.snap_steps[k]) { set_error("snapshot step not reached yet"); return BP_ERR_STATE; }
+    if (n < sh.snap_n) { set_error("host buffer too small"); return BP_ERR_ARG; }
+    SIM_CK(cudaStreamSynchronize(s->st));
+    SIM_CK(cudaMemcpy(host, sh.d_snap + off, sh.snap_n * 4, cudaMemcpyDeviceToHost));
+    return BP_OK;
+}
+
+int bp_get_dims(bp_sim* s, int* nxe, int* nye, int* nze) {
+    if (!s) { set_error("null sim"); return BP_ERR_ARG; }
+    if (nxe) *nxe = s->shot.desc.nx;
+    if (nye) *nye = s->shot.desc.ny;
+    if (nze) *nze = s->shot.desc.nz;
+    return BP_OK;
+}
+
+int bp_get_field_f64(bp_sim* s, int field, double* host, size_t n) {
+    if (!s || !host || field < 0 || field >= BP_NFIELDS) { set_error("bad arguments"); return BP_ERR_ARG; }
+    Shot& sh = s->shot;
+    if (!sh.desc.f[field]) { set_error("field not evolved in this dimension"); return BP_ERR_NOT_FOUND; }
+    const size_t cnt = (size_t)sh.desc.nx * sh.desc.ny * sh.desc.nz;
+    if (n < cnt) { set_error("host buffer too small"); return BP_ERR_ARG; }
+    SIM_CK(cudaSetDevice(s->device));
+    double* d = nullptr;
+    SIM_CK(cudaMalloc(&d, cnt * 8));
+    cudaError_t e = launch_field_f64(sh.cfg.precision, sh.d_desc, field, d, s->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, d, cnt * 8, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    cudaFree(d);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
+    return BP_OK;
+}
+
+int bp_get_field(bp_sim* s, int field, float* host, size_t n) {
+    if (!s || !host) { set_error("bad arguments"); return BP_ERR_ARG; }
+    const size_t cnt = (size_t)s->shot.desc.nx * s->shot.desc.ny * s->shot.desc.nz;
+    if (n < cnt) { set_error("host buffer too small"); return BP_ERR_ARG; }
+    std::vector<double> tmp(cnt);
+    int rc = bp_get_field_f64(s, field, tmp.data(), cnt);
+    if (rc) return rc;
+    for (size_t i = 0; i < cnt; i++) host[i] = (float)tmp[i];
+    return BP_OK;
+}
+
+int bp_get_coef(bp_sim* s, int which, float* host, size_t n) {
+    if (!s || !host || which < 0 || which >= VC_COUNT + TC_COUNT) { set_error("bad arguments"); return BP_ERR_ARG; }
+    Shot& sh = s->shot;
+    const size_t cnt = (size_t)sh.desc.nx * sh.desc.ny * sh.desc.nz;
+    if (n < cnt) { set_error("host buffer too small"); return BP_ERR_ARG; }
+    SIM_CK(cudaSetDevice(s->device));
+    float* d = nullptr;
+    SIM_CK(cudaMalloc(&d, cnt * 4));
+    cudaError_t e = launch_coef(sh.cfg.precision, sh.d_desc, which, d, s->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, d, cnt * 4, cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    cudaFree(d);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
+    return BP_OK;
+}
+
+int bp_field_energy(bp_sim* s, double* energy) {
+    if (!s || !energy) { set_error("bad arguments"); return BP_ERR_ARG; }
+    SIM_CK(cudaSetDevice(s->device));
+    Shot& sh = s->shot;
+    SIM_CK(launch_energy(sh.cfg.precision, sh.d_desc, sh.d_scratch, sh.d_out, s->st));
+    SIM_CK(cudaMemcpyAsync(energy, sh.d_out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    SIM_CK(cudaStreamSynchronize(s->st));
+    return BP_OK;
+}
+
+int bp_get_scaling(bp_sim* s, int* em, int* es, float* dyn_scale, double* kmax, double* rmax) {
+    if (!s) { set_error("null sim"); return BP_ERR_ARG; }
+    Shot& sh = s->shot;
+    if (em) *em = sh.em;
+    if (es) *es = sh.es;
+    if (dyn_scale) {
+        int it = sh.it_host;
+        *dyn_scale = sh.dyn.empty() ? 1.0f : sh.dyn[it > 0 ? std::min(it - 1, (int)sh.dyn.size() - 1) : 0];
+    }
+    if (kmax) *kmax = sh.kmax;
+    if (rmax) *rmax = sh.rmax;
+    return BP_OK;
+}
+
+int bp_profile_phases(bp_sim* s, int nsteps, float ms[3]) {
+    if (!s || !ms || nsteps < 1) { set_error("bad arguments"); return BP_ERR_ARG; }
+    SIM_CK(cudaSetDevice(s->device));
+    Shot& sh = s->shot;
+    Runner& R = s->run;
+    nsteps = std::min(nsteps, sh.cfg.nt - sh.it_host);
+    if (nsteps < 1) { set_error("no steps left to profile"); return BP_ERR_STATE; }
+    cudaEvent_t ev[4];
+    for (auto& x : ev) SIM_CK(cudaEventCreate(&x));
+    double acc[3] = {0, 0, 0};
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < nsteps && e == cudaSuccess; i++) {
+        cudaEventRecord(ev[0], s->st);
+        e = launch_phase(R.prec, R.dim, R.order, true, R.d_shots, R.nshots, R.ntiles, 0, R.grid_v, s->st);
+        cudaEventRecord(ev[1], s->st);
+        if (e == cudaSuccess) e = launch_phase(R.prec, R.dim, R.order, false, R.d_shots, R.nshots, R.ntiles, 0, R.grid_t, s->st);
+        cudaEventRecord(ev[2], s->st);
+        if (e == cudaSuccess) e = launch_post(R.prec, R.d_shots, R.nshots, R.max_rec, 0, 1, s->st);
+        if (e == cudaSuccess) e = launch_advance(R.d_shots, R.nshots, 1, s->st);
+        cudaEventRecord(ev[3], s->st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[3]);
+        float t;
+        for (int q = 0; q < 3 && e == cudaSuccess; q++) {
+            cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+            acc[q] += t;
+        }
+        R.launches += 4;
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
+    sh.it_host += nsteps;
+    for (int q = 0; q < 3; q++) ms[q] = (float)(acc[q] / nsteps);
+    return BP_OK;
+}
+
+int bp_algorithmic_bytes(bp_sim* s, double bpc[2], long long* cells) {
+    if (!s || !bpc) { set_error("bad arguments"); return BP_ERR_ARG; }
+    const bp_config& c = s->shot.cfg;
+    // words touched once per phase per updated cell (each array element once;
+    // neighbour re-reads and the slab-only CPML variables not counted):
+    //   V: read stresses+p, read+write vu,vw, read coefficients
+    //   T: read vu,vw, read+write stresses+p, read coefficients
+    double fb, cb;
+    if (c.precision == BP_PREC_FP64) { fb = 8; cb = 8; }
+    else if (c.precision == BP_PREC_FP32) { fb = 4; cb = 4; }
+    else { fb = 3; cb = c.comp_coef_lo ? 3 : 2; }
+    if (c.dim == 3) {
+        bpc[0] = (7 + 2 * 6) * fb + 10 * cb;
+        bpc[1] = (6 + 2 * 7) * fb + 7 * cb;
+    } else {
+        bpc[0] = (4 + 2 * 4) * fb + 7 * cb;
+        bpc[1] = (4 + 2 * 4) * fb + 5 * cb;
+    }
+    if (cells) *cells = s->shot.cells;
+    return BP_OK;
+}
+
+int bp_launches_per_step(bp_sim* s, int* n) {
+    if (!s || !n) { set_error("bad arguments"); return BP_ERR_ARG; }
+    *n = 3;
+    return BP_OK;
+}
+
+int bp_launch_count(bp_sim* s, long long* n) {
+    if (!s || !n) { set_error("bad arguments"); return BP_ERR_ARG; }
+    *n = s->run.launches;
+    return BP_OK;
+}
+
+int bp_rel_l2_device(const float* d_x, const float* d_ref, size_t n, double* rel) {
+    if (!d_x || !d_ref || !rel) { set_error("bad arguments"); return BP_ERR_ARG; }
+    const int nb = reduce_blocks();
+    double* scratch = nullptr;
+    SIM_CK(cudaMalloc(&scratch, (2 * (size_t)nb + 2) * sizeof(double)));
+    double h[2] = {0, 0};
+    cudaError_t e = launch_rel_l2(d_x, d_ref, (long long)n, scratch, scratch + 2 * nb, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(h, scratch + 2 * nb, 2 * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(scratch);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
+    *rel = h[1] > 0 ? std::sqrt(h[0] / h[1]) : std::sqrt(h[0]);
+    return BP_OK;
+}
+
+int bp_trace_rel_l2(bp_sim* x, bp_sim* ref, int comp, double* rel) {
+    if (!x || !ref || !rel || comp < 0 || comp >= BP_NTRACE) { set_error("bad arguments"); return BP_ERR_ARG; }
+    if (x->shot.nurec != ref->shot.nurec || x->shot.cfg.nt != ref->shot.cfg.nt) { set_error("traces differ in shape"); return BP_ERR_ARG; }
+    SIM_CK(cudaStreamSynchronize(x->st));
+    SIM_CK(cudaStreamSynchronize(ref->st));
+    const size_t n = (size_t)x->shot.nurec * x->shot.cfg.nt;
+    return bp_rel_l2_device(x->shot.desc.traces + comp * n, ref->shot.desc.traces + comp * n, n, rel);
+}
+
+void bp_destroy(bp_sim* s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    if (s->st) cudaStreamSynchronize(s->st);
+    s->run.reset_graph();
+    s->shot.destroy();
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+}
+
+// ---- reference-format text output (Float/main.cu:1501-1516,1563-1588) ----
+static int write_rows(const std::string& path, const float* data, int nr, int nc) {
+    FILE* fp = fopen(path.c_str(), "wt");
+    if (!fp) { set_error("cannot open " + path); return BP_ERR_ARG; }
+    for (int i = 0; i < nr; i++) {
+        for (int j = 0; j < nc; j++) {
+            fprintf(fp, "%e ", data[(size_t)i * nc + j]);
+            if ((j + 1) % nc == 0) fprintf(fp, "\n");
+        }
+        fprintf(fp, "\n");
+    }
+    fclose(fp);
+    return BP_OK;
+}
+
+int bp_write_reference_outputs(bp_sim* s, const char* dir) {
+    if (!s || !dir) { set_error("bad arguments"); return BP_ERR_ARG; }
+    mkdir(dir, 0755);
+    Shot& sh = s->shot;
+    const int nt = sh.cfg.nt, nr = sh.cfg.nrec;
+    const std::string d(dir);
+    const char* sis[BP_NTRACE] = {"sisx.dat", "sisz.dat", "sisvu.dat", "sisvw.dat", "sisp.dat"};
+    std::vector<float> buf((size_t)nr * nt);
+    for (int c = 0; c < BP_NTRACE; c++) {
+        int rc = bp_get_traces(s, c, buf.data(), buf.size());
+        if (rc) return rc;
+        rc = write_rows(d + "/" + sis[c], buf.data(), nr, nt);
+        if (rc) return rc;
+    }
+    const int nx = sh.desc.nx, ny = sh.desc.ny, nz = sh.desc.nz;
+    const bool slice = sh.cfg.dim == 3 && sh.cfg.snap_y >= 0;
+    std::vector<float> snap(sh.snap_n), sl((size_t)nx * nz);
+    for (int k = 0; k < (int)sh.snap_steps.size(); k++) {
+        for (int f = 0; f < BP_NFIELDS; f++) {
+            if (sh.snap_off[(size_t)k * BP_NFIELDS + f] < 0) continue;
+            int rc = bp_get_snapshot(s, k, f, snap.data(), snap.size());
+            if (rc) return rc;
+            const float* src = snap.data();
+            if (!slice && sh.cfg.dim == 3) {   // full volume: write the y = NY/2 slice like wfile3d
+                for (int z = 0; z < nz; z++)
+                    for (int x = 0; x < nx; x++) sl[(size_t)z * nx + x] = snap[(size_t)x + (size_t)(ny / 2) * nx + (size_t)z * nx * ny];
+                src = sl.data();
+            }
+            rc = write_rows(d + "/" + kFieldNames[f] + std::to_string(sh.snap_steps[k]) + ".dat", src, nz, nx);
+            if (rc) return rc;
+        }
+    }
+    // final txx (Float/main.cu:1166-1175,1190)
+    std::vector<float> full((size_t)nx * ny * nz);
+    int rc = bp_get_field(s, BP_F_TXX, full.data(), full.size());
+    if (rc) return rc;
+    int jy = sh.cfg.dim == 3 ? ny / 2 : 0;
+    for (int z = 0; z < nz; z++)
+        for (int x = 0; x < nx; x++) sl[(size_t)z * nx + x] = full[(size_t)x + (size_t)jy * nx + (size_t)z * nx * ny];
+    return write_rows(d + "/txx.dat", sl.data(), nz, nx);
+}
+
+}  // extern "C"

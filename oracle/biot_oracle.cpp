@@ -1,0 +1,882 @@
+// biot_oracle.cpp - CPU restatement of the reference Biot/CPML stepper.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the oracle: only tests/, the
+// smoke check in __graft_entry__.py and the CPU-baseline leg of bench.py load
+// it, and only to check or time against the CUDA library.  Nothing in the
+// product (mixedprecisionfaracoustic_b200/) links it.
+//
+// What it restates (file:line in the reference project):
+//   * create_model            Float/main.cu:1590-1655  (orc_medium_reference_borehole)
+//   * extmodel edge padding   Float/main.cu:1662-1794  (clamp-to-edge, pad_index)
+//   * staggered averaging     Float/main.cu:472-513    (Oracle::build_coefficients)
+//   * CPML profiles           Float/main.cu:570-654    (Oracle::build_profiles)
+//   * Ricker source           Float/main.cu:1050-1062  (ricker_ref)
+//   * Source kernel           Float/main.cu:45-59      (Oracle::inject)
+//   * FD_V kernel             Float/main.cu:64-192     (Oracle::v_phase)
+//   * FD_T kernel             Float/main.cu:194-295    (Oracle::t_phase)
+//   * trace/snapshot capture  Float/main.cu:1075-1163
+//   * compensated codec       Half/main.cu:59-100      (orc_store_ch / orc_load_ch)
+//   * exponent scaling scan   Half/main.cu:745-843     (orc_comp16_exponents)
+//
+// Modes
+//   ORC_REF32 (0): float storage with the reference's exact C type promotions
+//                  (the double literal 0.5 in FD_V/FD_T, Float/main.cu:106-113,
+//                  130-158, 252-285) and no FMA contraction (-ffp-contract=off).
+//   ORC_FP64  (1): the same equations in double precision from the same float
+//                  medium: the accuracy reference ("FP64 oracle").
+//
+// Generalisations beyond the reference (which is 3D, order 2 only):
+//   * dim 2: the x-z restriction of the same equations (all y derivatives and
+//     the y components dropped; tyy is not evolved).
+//   * order 4: D f = (9/8 (f1 - f0) - 1/24 (f2 - f_-1)) / H on the same
+//     staggering; update region shrinks to [2, N-3] per axis.
+//   * ψ/prev updates are skipped where the axis profile is inactive (d == 0,
+//     e == 1); in the reference they leave ψ exactly 0 there, so this is exact.
+#include "../include/biot.h"
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+#include <xmmintrin.h>
+
+namespace {
+
+enum { ORC_REF32 = 0, ORC_FP64 = 1 };
+
+// Medium array order inside bp_medium.
+enum { M_RHO, M_RHOF, M_M, M_C, M_H, M_H2MU, M_MU, M_C1, M_C2, M_COUNT };
+
+// Derivative slots.  Forward differences use the half-grid profile (d2/e2),
+// backward differences the integer-grid profile (d/e): this is the pairing of
+// every ψ array with its profile in Float/main.cu:130-153 and :252-285.
+struct Slot {
+    int field;    // BP_F_* differentiated
+    int axis;     // 0 x, 1 y, 2 z
+    int forward;  // 1: f(i+1)-f(i) (half grid), 0: f(i)-f(i-1) (integer grid)
+};
+// V phase (Float/main.cu:115-128): x1 x2 x3 s1 y1 y2 y3 s2 z1 z2 z3 s3
+const Slot kVSlots[12] = {
+    {BP_F_TXX, 0, 1}, {BP_F_TXY, 1, 0}, {BP_F_TXZ, 2, 0}, {BP_F_P, 0, 1},
+    {BP_F_TYY, 1, 1}, {BP_F_TXY, 0, 0}, {BP_F_TYZ, 2, 0}, {BP_F_P, 1, 1},
+    {BP_F_TZZ, 2, 1}, {BP_F_TXZ, 0, 0}, {BP_F_TYZ, 1, 0}, {BP_F_P, 2, 1}};
+// T phase (Float/main.cu:234-249): uxx uyy uzz wx wy wz uxy uyx uxz uzx uyz uzy
+const Slot kTSlots[12] = {
+    {BP_F_VUX, 0, 0}, {BP_F_VUY, 1, 0}, {BP_F_VUZ, 2, 0},
+    {BP_F_VWX, 0, 0}, {BP_F_VWY, 1, 0}, {BP_F_VWZ, 2, 0},
+    {BP_F_VUX, 1, 1}, {BP_F_VUY, 0, 1}, {BP_F_VUX, 2, 1},
+    {BP_F_VUZ, 0, 1}, {BP_F_VUY, 2, 1}, {BP_F_VUZ, 1, 1}};
+
+inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// Ricker wavelet exactly as the reference host code evaluates it
+// (Float/main.cu:1050,1059: float tt, float T0, double PI literal, double exp).
+float ricker_ref(int it, float DT, float F0, float T0) {
+    const double PI = 3.1415926535;
+    float tt = it * DT;
+    float a = tt - T0;
+    double v = -(1 - 2 * PI * PI * F0 * F0 * a * a) * exp(-PI * PI * F0 * F0 * a * a);
+    return (float)v;
+}
+double ricker_f64(int it, double DT, double F0, double T0) {
+    const double PI = 3.1415926535;
+    double a = it * DT - T0;
+    return -(1 - 2 * PI * PI * F0 * F0 * a * a) * exp(-PI * PI * F0 * F0 * a * a);
+}
+
+struct Profile {            // one axis, padded length n
+    std::vector<float> d, e, d2, e2;      // reference float tables
+    std::vector<double> dd, ed, dd2, ed2; // FP64 tables
+    std::vector<unsigned char> act, act2; // profile active (d != 0)
+};
+
+// CPML profile of one axis, Float/main.cu:570-654 with its float region tests.
+void build_profile_axis(Profile& p, int n, int np, float H, float DT, float v0f, float RCf) {
+    p.d.assign(n, 0.0f); p.d2.assign(n, 0.0f);
+    p.e.assign(n, 1.0f); p.e2.assign(n, 1.0f);
+    p.dd.assign(n, 0.0); p.dd2.assign(n, 0.0);
+    p.ed.assign(n, 1.0); p.ed2.assign(n, 1.0);
+    float DP = np * H;
+    float oleft = DP;
+    float oright = (n - 1) * H - DP;
+    float RC = RCf;
+    float v0 = v0f;
+    float d0 = 3.0 * v0 * log(1.0 / RC) / (2.0 * DP);
+    double d0d = 3.0 * (double)v0 * log(1.0 / (double)RC) / (2.0 * (double)DP);
+    double Hd = H, DPd = DP, DTd = DT;
+    for (int i = 0; i < n; i++) {
+        float x = i * H;
+        double xd = i * Hd;
+        if (x >= 0 && x < oleft) {
+            p.d[i] = d0 * pow(((oleft - x) / DP), 2);
+            p.d2[i] = d0 * pow(((oleft - x - 0.5 * H) / DP), 2);
+            p.e[i] = std::exp(-(p.d[i]) * DT);
+            p.e2[i] = std::exp(-(p.d2[i]) * DT);
+            double a = ((double)oleft - xd) / DPd, b = ((double)oleft - xd - 0.5 * Hd) / DPd;
+            p.dd[i] = d0d * a * a;
+            p.dd2[i] = d0d * b * b;
+        }
+        if (x >= oright && x < n * H) {
+            p.d[i] = d0 * pow(((x - oright) / DP), 2);
+            p.d2[i] = d0 * pow(((x + 0.5 * H - oright) / DP), 2);
+            p.e[i] = std::exp((-p.d[i]) * DT);
+            p.e2[i] = std::exp((-p.d2[i]) * DT);
+            double a = (xd - (double)oright) / DPd, b = (xd + 0.5 * Hd - (double)oright) / DPd;
+            p.dd[i] = d0d * a * a;
+            p.dd2[i] = d0d * b * b;
+        }
+        p.ed[i] = exp(-p.dd[i] * DTd);
+        p.ed2[i] = exp(-p.dd2[i] * DTd);
+    }
+    p.act.resize(n); p.act2.resize(n);
+    for (int i = 0; i < n; i++) {
+        p.act[i] = (p.d[i] != 0.0f || p.e[i] != 1.0f || p.dd[i] != 0.0) ? 1 : 0;
+        p.act2[i] = (p.d2[i] != 0.0f || p.e2[i] != 1.0f || p.dd2[i] != 0.0) ? 1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+template <typename T, bool REF>
+struct Oracle {
+    bp_config cfg{};
+    int dim = 3, order = 2, hw = 1;
+    int nx = 0, ny = 1, nz = 0;       // padded extents
+    size_t sy = 0, sz = 0, ncell = 0; // strides
+    float H = 0, DT = 0, F0 = 0, T0 = 0;
+    double Hd = 0, DTd = 0, F0d = 0, T0d = 0;
+    int it = 0;
+
+    std::vector<T> f[BP_NFIELDS];
+    // coefficients at cell (staggered positions as in the reference)
+    std::vector<T> rhox, rhoy, rhoz, rhof, C1x, C1y, C1z, C2x, C2y, C2z;
+    std::vector<T> cC, cM, cH, cH2u, muxy, muxz, muyz;
+    std::vector<T> psiV[12], prevV[12], psiT[12], prevT[12];
+    Profile prof[3];
+
+    std::vector<int> rec_idx;
+    std::vector<float> traces;       // [comp][rec][nt]
+    std::vector<int> snap_steps;
+    std::vector<unsigned> snap_masks;
+    std::vector<std::vector<float>> snaps;  // [k*13 + field]
+    size_t snap_n = 0;
+    int src_idx = -1;
+
+    bool active_slot(const Slot& s) const { return dim == 3 || s.axis != 1; }
+    bool field_used(int fidx) const {
+        if (dim == 3) return true;
+        return !(fidx == BP_F_VUY || fidx == BP_F_VWY || fidx == BP_F_TYY ||
+                 fidx == BP_F_TXY || fidx == BP_F_TYZ);
+    }
+    size_t stride(int axis) const { return axis == 0 ? 1 : (axis == 1 ? sy : sz); }
+
+    int setup(const bp_config* c, const bp_medium* m) {
+        cfg = *c;
+        dim = c->dim; order = c->order; hw = order / 2;
+        nx = c->nx + 2 * c->npml;
+        ny = dim == 3 ? c->ny + 2 * c->npml : 1;
+        nz = c->nz + 2 * c->npml;
+        sy = nx; sz = (size_t)nx * ny; ncell = sz * nz;
+        H = c->dx; DT = c->dt; F0 = c->f0;
+        T0 = c->t0 > 0 ? c->t0 : (float)(1.2 / F0);
+        Hd = H; DTd = DT; F0d = F0; T0d = c->t0 > 0 ? (double)c->t0 : 1.2 / F0d;
+        for (int i = 0; i < BP_NFIELDS; i++)
+            if (field_used(i)) f[i].assign(ncell, T(0));
+        build_coefficients(m);
+        build_profile_axis(prof[0], nx, c->npml, H, DT, c->pml_v0, c->pml_r);
+        if (dim == 3) build_profile_axis(prof[1], ny, c->npml, H, DT, c->pml_v0, c->pml_r);
+        build_profile_axis(prof[2], nz, c->npml, H, DT, c->pml_v0, c->pml_r);
+        for (int s = 0; s < 12; s++) {
+            if (active_slot(kVSlots[s])) { psiV[s].assign(ncell, T(0)); prevV[s].assign(ncell, T(0)); }
+            if (active_slot(kTSlots[s])) { psiT[s].assign(ncell, T(0)); prevT[s].assign(ncell, T(0)); }
+        }
+        src_idx = c->src_x + (dim == 3 ? c->src_y * (int)sy : 0) + c->src_z * (int)sz;
+        rec_idx.resize(c->nrec);
+        for (int r = 0; r < c->nrec; r++)
+            rec_idx[r] = c->rec_x[r] + (dim == 3 ? c->rec_y[r] * (int)sy : 0) + c->rec_z[r] * (int)sz;
+        traces.assign((size_t)BP_NTRACE * c->nrec * c->nt, 0.0f);
+        snap_steps.assign(c->snap_steps, c->snap_steps + c->nsnap);
+        snap_masks.resize(c->nsnap);
+        for (int k = 0; k < c->nsnap; k++)
+            snap_masks[k] = c->snap_masks ? c->snap_masks[k] : c->snap_fields;
+        snap_n = (dim == 3 && c->snap_y >= 0) ? (size_t)nx * nz : ncell;
+        snaps.assign((size_t)c->nsnap * BP_NFIELDS, std::vector<float>());
+        return 0;
+    }
+
+    // extmodel (Float/main.cu:1662-1794) is clamp-to-edge padding.
+    float padded(const float* a, int x, int y, int z) const {
+        int np = cfg.npml;
+        int px = clampi(x - np, 0, cfg.nx - 1);
+        int pz = clampi(z - np, 0, cfg.nz - 1);
+        int py = dim == 3 ? clampi(y - np, 0, cfg.ny - 1) : 0;
+        int pnx = cfg.nx, pny = dim == 3 ? cfg.ny : 1;
+        return a[(size_t)px + (size_t)py * pnx + (size_t)pz * pnx * pny];
+    }
+
+    // Harmonic 4-point shear average (Float/main.cu:480-491).
+    T harm4(float a, float b, float c, float d) const {
+        if (a == 0 || b == 0 || c == 0 || d == 0) return T(0);
+        if (REF) return (T)(1 / (0.25 * (1 / a + 1 / b + 1 / c + 1 / d)));
+        double s = 1.0 / a + 1.0 / b + 1.0 / c + 1.0 / d;
+        return (T)(1.0 / (0.25 * s));
+    }
+    T inv2(float a, float b) const {      // rho_temp = 2 / (rho_i + rho_i+1)
+        if (REF) return (T)(2 / (a + b));
+        return (T)(2.0 / ((double)a + (double)b));
+    }
+    T avg2(float a, float b) const {      // 0.5 * (C_i + C_i+1)
+        if (REF) return (T)(0.5 * (a + b));
+        return (T)(0.5 * ((double)a + (double)b));
+    }
+
+    void build_coefficients(const bp_medium* m) {
+        const float* A[M_COUNT] = {m->rho, m->rhof, m->M, m->C, m->H, m->H2mu, m->mu, m->C1, m->C2};
+        auto alloc = [&](std::vector<T>& v) { v.assign(ncell, T(0)); };
+        alloc(rhox); alloc(rhoz); alloc(rhof); alloc(C1x); alloc(C1z); alloc(C2x); alloc(C2z);
+        alloc(cC); alloc(cM); alloc(cH); alloc(cH2u); alloc(muxz);
+        if (dim == 3) { alloc(rhoy); alloc(C1y); alloc(C2y); alloc(muxy); alloc(muyz); }
+        // cell-centred moduli are the padded arrays themselves
+        for (int z = 0; z < nz; z++)
+            for (int y = 0; y < ny; y++)
+                for (int x = 0; x < nx; x++) {
+                    size_t i = x + y * sy + z * sz;
+                    rhof[i] = padded(A[M_RHOF], x, y, z);
+                    cC[i] = padded(A[M_C], x, y, z);
+                    cM[i] = padded(A[M_M], x, y, z);
+                    cH[i] = padded(A[M_H], x, y, z);
+                    cH2u[i] = padded(A[M_H2MU], x, y, z);
+                }
+        // staggered averages over the interior 1..N-2 (Float/main.cu:473-477)
+        int ylo = dim == 3 ? 1 : 0, yhi = dim == 3 ? ny - 1 : 1;
+#pragma omp parallel for schedule(static)
+        for (int z = 1; z < nz - 1; z++)
+            for (int y = ylo; y < yhi; y++)
+                for (int x = 1; x < nx - 1; x++) {
+                    size_t i = x + y * sy + z * sz;
+                    const float* mu = A[M_MU];
+                    const float* rho = A[M_RHO];
+                    muxz[i] = harm4(padded(mu, x, y, z), padded(mu, x + 1, y, z),
+                                    padded(mu, x, y, z + 1), padded(mu, x + 1, y, z + 1));
+                    rhox[i] = inv2(padded(rho, x, y, z), padded(rho, x + 1, y, z));
+                    rhoz[i] = inv2(padded(rho, x, y, z), padded(rho, x, y, z + 1));
+                    C1x[i] = avg2(padded(A[M_C1], x, y, z), padded(A[M_C1], x + 1, y, z));
+                    C1z[i] = avg2(padded(A[M_C1], x, y, z), padded(A[M_C1], x, y, z + 1));
+                    C2x[i] = avg2(padded(A[M_C2], x, y, z), padded(A[M_C2], x + 1, y, z));
+                    C2z[i] = avg2(padded(A[M_C2], x, y, z), padded(A[M_C2], x, y, z + 1));
+                    if (dim == 3) {
+                        muyz[i] = harm4(padded(mu, x, y, z), padded(mu, x, y + 1, z),
+                                        padded(mu, x, y, z + 1), padded(mu, x, y + 1, z + 1));
+                        muxy[i] = harm4(padded(mu, x, y, z), padded(mu, x + 1, y, z),
+                                        padded(mu, x, y + 1, z), padded(mu, x + 1, y + 1, z));
+                        rhoy[i] = inv2(padded(rho, x, y, z), padded(rho, x, y + 1, z));
+                        C1y[i] = avg2(padded(A[M_C1], x, y, z), padded(A[M_C1], x, y + 1, z));
+                        C2y[i] = avg2(padded(A[M_C2], x, y, z), padded(A[M_C2], x, y + 1, z));
+                    }
+                }
+    }
+
+    // CPML memory update (Float/main.cu:130): ψ = ψ e + (-DT d 0.5)(e prev + ∂); prev = ∂; ∂ += ψ
+    inline T cpml(T& psi, T& prev, T dv, int axis, int fwd, int idx) const {
+        const Profile& p = prof[axis];
+        if (REF) {
+            float d = fwd ? p.d2[idx] : p.d[idx];
+            float e = fwd ? p.e2[idx] : p.e[idx];
+            float ps = (float)psi, pv = (float)prev, x = (float)dv;
+            float nps = (float)((double)(ps * e) + ((double)(-DT * d) * 0.5) * (double)(e * pv + x));
+            psi = (T)nps; prev = dv;
+            return (T)(x + nps);
+        } else {
+            double d = fwd ? p.dd2[idx] : p.dd[idx];
+            double e = fwd ? p.ed2[idx] : p.ed[idx];
+            double nps = (double)psi * e + (-DTd * d * 0.5) * (e * (double)prev + (double)dv);
+            psi = (T)nps; prev = dv;
+            return (T)((double)dv + nps);
+        }
+    }
+
+    void inject() {
+        if (src_idx < 0) return;
+        T I;
+        if (REF) I = (T)ricker_ref(it, DT, F0, T0);
+        else I = (T)ricker_f64(it, DTd, F0d, T0d);
+        if (cfg.src_mask & BP_SRC_TAU) {
+            f[BP_F_TXX][src_idx] = f[BP_F_TXX][src_idx] + I;
+            if (dim == 3) f[BP_F_TYY][src_idx] = f[BP_F_TYY][src_idx] + I;
+            f[BP_F_TZZ][src_idx] = f[BP_F_TZZ][src_idx] + I;
+        }
+        if (cfg.src_mask & BP_SRC_P) f[BP_F_P][src_idx] = f[BP_F_P][src_idx] - I;
+    }
+
+    // staggered derivative along stride st; ORD known at compile time
+    template <int ORD, bool FWD>
+    inline T D(const T* a, size_t i, size_t st) const {
+        const T h = REF ? (T)H : (T)Hd;
+        if (ORD == 2) return FWD ? (a[i + st] - a[i]) / h : (a[i] - a[i - st]) / h;
+        const T c1 = REF ? (T)1.125f : (T)1.125;
+        const T c2 = REF ? (T)(-1.0f / 24.0f) : (T)(-1.0 / 24.0);
+        if (FWD) return (c1 * (a[i + st] - a[i]) + c2 * (a[i + 2 * st] - a[i - st])) / h;
+        return (c1 * (a[i] - a[i - st]) + c2 * (a[i + st] - a[i - 2 * st])) / h;
+    }
+    // FD_V restated (Float/main.cu:103-191) for one row of cells
+    template <int DIM, int ORD>
+    void v_row(int y, int z) {
+        const size_t base = (size_t)y * sy + (size_t)z * sz;
+        const T* txx = f[BP_F_TXX].data(); const T* tzz = f[BP_F_TZZ].data();
+        const T* txz = f[BP_F_TXZ].data(); const T* pp = f[BP_F_P].data();
+        const T* tyy = DIM == 3 ? f[BP_F_TYY].data() : nullptr;
+        const T* txy = DIM == 3 ? f[BP_F_TXY].data() : nullptr;
+        const T* tyz = DIM == 3 ? f[BP_F_TYZ].data() : nullptr;
+        const Profile &px = prof[0], &py = prof[1], &pz = prof[2];
+        const bool yf = DIM == 3 && py.act2[y], yb = DIM == 3 && py.act[y];
+        const bool zf = pz.act2[z], zb = pz.act[z];
+        for (int x = hw; x < nx - hw; x++) {
+            const size_t i = base + x;
+            T x1 = D<ORD, true>(txx, i, 1), s1 = D<ORD, true>(pp, i, 1), z2 = D<ORD, false>(txz, i, 1);
+            T x3 = D<ORD, false>(txz, i, sz), z1 = D<ORD, true>(tzz, i, sz), s3 = D<ORD, true>(pp, i, sz);
+            T x2 = 0, y1 = 0, y2 = 0, y3 = 0, z3 = 0, s2 = 0;
+            if (DIM == 3) {
+                x2 = D<ORD, false>(txy, i, sy); y1 = D<ORD, true>(tyy, i, sy); y2 = D<ORD, false>(txy, i, 1);
+                y3 = D<ORD, false>(tyz, i, sz); z3 = D<ORD, false>(tyz, i, sy); s2 = D<ORD, true>(pp, i, sy);
+            }
+            if (px.act2[x]) {
+                x1 = cpml(psiV[0][i], prevV[0][i], x1, 0, 1, x);
+                s1 = cpml(psiV[3][i], prevV[3][i], s1, 0, 1, x);
+            }
+            if (px.act[x]) {
+                if (DIM == 3) y2 = cpml(psiV[5][i], prevV[5][i], y2, 0, 0, x);
+                z2 = cpml(psiV[9][i], prevV[9][i], z2, 0, 0, x);
+            }
+            if (DIM == 3) {
+                if (yb) { x2 = cpml(psiV[1][i], prevV[1][i], x2, 1, 0, y); z3 = cpml(psiV[10][i], prevV[10][i], z3, 1, 0, y); }
+                if (yf) { y1 = cpml(psiV[4][i], prevV[4][i], y1, 1, 1, y); s2 = cpml(psiV[7][i], prevV[7][i], s2, 1, 1, y); }
+            }
+            if (zb) {
+                x3 = cpml(psiV[2][i], prevV[2][i], x3, 2, 0, z);
+                if (DIM == 3) y3 = cpml(psiV[6][i], prevV[6][i], y3, 2, 0, z);
+            }
+            if (zf) {
+                z1 = cpml(psiV[8][i], prevV[8][i], z1, 2, 1, z);
+                s3 = cpml(psiV[11][i], prevV[11][i], s3, 2, 1, z);
+            }
+            T sx, sy_, szz;
+            if (DIM == 3) { sx = x1 + x2 + x3; sy_ = y1 + y2 + y3; szz = z1 + z2 + z3; }
+            else { sx = x1 + x3; sy_ = T(0); szz = z1 + z2; }
+            update_v_axis(i, sx, s1, rhox[i], C1x[i], C2x[i], BP_F_VUX, BP_F_VWX);
+            if (DIM == 3) update_v_axis(i, sy_, s2, rhoy[i], C1y[i], C2y[i], BP_F_VUY, BP_F_VWY);
+            update_v_axis(i, szz, s3, rhoz[i], C1z[i], C2z[i], BP_F_VUZ, BP_F_VWZ);
+        }
+    }
+
+    // vw semi-implicit friction update and vu update (Float/main.cu:106-113,160-190)
+    inline void update_v_axis(size_t i, T sum, T dp, T rho, T C1, T C2, int fu, int fw) {
+        T rf = rhof[i];
+        T vw_old = f[fw][i];
+        T vw_new;
+        if (REF) {
+            float r = (float)rho, c1 = (float)C1, c2 = (float)C2, rff = (float)rf;
+            float CC1 = 0.5 * c1 * DT + c2 - rff * rff * r;
+            float CC2 = c2 - rff * rff * r - 0.5 * c1 * DT;
+            float su = (float)sum, s = (float)dp, vw = (float)vw_old;
+            float nv;
+            if (c1 == 0.0f) nv = 0.0f;
+            else nv = (vw * CC2 - DT * (rff * r * su + s)) / CC1;
+            float vu = (float)f[fu][i];
+            vu = vu + DT * r * su - rff * r * (nv - vw);
+            vw_new = (T)nv;
+            f[fu][i] = (T)vu;
+        } else {
+            double CC1 = 0.5 * (double)C1 * DTd + (double)C2 - (double)rf * (double)rf * (double)rho;
+            double CC2 = (double)C2 - (double)rf * (double)rf * (double)rho - 0.5 * (double)C1 * DTd;
+            double nv;
+            if ((double)C1 == 0.0) nv = 0.0;
+            else nv = ((double)vw_old * CC2 - DTd * ((double)rf * (double)rho * (double)sum + (double)dp)) / CC1;
+            double vu = (double)f[fu][i];
+            vu = vu + DTd * (double)rho * (double)sum - (double)rf * (double)rho * (nv - (double)vw_old);
+            vw_new = (T)nv;
+            f[fu][i] = (T)vu;
+        }
+        f[fw][i] = vw_new;
+    }
+
+    // FD_T restated (Float/main.cu:232-294) for one row of cells
+    template <int DIM, int ORD>
+    void t_row(int y, int z) {
+        const size_t base = (size_t)y * sy + (size_t)z * sz;
+        const T* vux = f[BP_F_VUX].data(); const T* vuz = f[BP_F_VUZ].data();
+        const T* vwx = f[BP_F_VWX].data(); const T* vwz = f[BP_F_VWZ].data();
+        const T* vuy = DIM == 3 ? f[BP_F_VUY].data() : nullptr;
+        const T* vwy = DIM == 3 ? f[BP_F_VWY].data() : nullptr;
+        T* P = f[BP_F_P].data(); T* TXX = f[BP_F_TXX].data(); T* TZZ = f[BP_F_TZZ].data(); T* TXZ = f[BP_F_TXZ].data();
+        T* TYY = DIM == 3 ? f[BP_F_TYY].data() : nullptr;
+        T* TXY = DIM == 3 ? f[BP_F_TXY].data() : nullptr;
+        T* TYZ = DIM == 3 ? f[BP_F_TYZ].data() : nullptr;
+        const Profile &px = prof[0], &py = prof[1], &pz = prof[2];
+        const bool yf = DIM == 3 && py.act2[y], yb = DIM == 3 && py.act[y];
+        const bool zf = pz.act2[z], zb = pz.act[z];
+        const T dt = REF ? (T)DT : (T)DTd;
+        for (int x = hw; x < nx - hw; x++) {
+            const size_t i = base + x;
+            T uxx = D<ORD, false>(vux, i, 1), wx = D<ORD, false>(vwx, i, 1), uzx = D<ORD, true>(vuz, i, 1);
+            T uzz = D<ORD, false>(vuz, i, sz), wz = D<ORD, false>(vwz, i, sz), uxz = D<ORD, true>(vux, i, sz);
+            T uyy = 0, wy = 0, uxy = 0, uyx = 0, uyz = 0, uzy = 0;
+            if (DIM == 3) {
+                uyy = D<ORD, false>(vuy, i, sy); wy = D<ORD, false>(vwy, i, sy); uxy = D<ORD, true>(vux, i, sy);
+                uyx = D<ORD, true>(vuy, i, 1); uyz = D<ORD, true>(vuy, i, sz); uzy = D<ORD, true>(vuz, i, sy);
+            }
+            if (px.act[x]) {
+                uxx = cpml(psiT[0][i], prevT[0][i], uxx, 0, 0, x);
+                wx = cpml(psiT[3][i], prevT[3][i], wx, 0, 0, x);
+            }
+            if (px.act2[x]) {
+                if (DIM == 3) uyx = cpml(psiT[7][i], prevT[7][i], uyx, 0, 1, x);
+                uzx = cpml(psiT[9][i], prevT[9][i], uzx, 0, 1, x);
+            }
+            if (DIM == 3) {
+                if (yb) { uyy = cpml(psiT[1][i], prevT[1][i], uyy, 1, 0, y); wy = cpml(psiT[4][i], prevT[4][i], wy, 1, 0, y); }
+                if (yf) { uxy = cpml(psiT[6][i], prevT[6][i], uxy, 1, 1, y); uzy = cpml(psiT[11][i], prevT[11][i], uzy, 1, 1, y); }
+            }
+            if (zb) {
+                uzz = cpml(psiT[2][i], prevT[2][i], uzz, 2, 0, z);
+                wz = cpml(psiT[5][i], prevT[5][i], wz, 2, 0, z);
+            }
+            if (zf) {
+                uxz = cpml(psiT[8][i], prevT[8][i], uxz, 2, 1, z);
+                if (DIM == 3) uyz = cpml(psiT[10][i], prevT[10][i], uyz, 2, 1, z);
+            }
+            const T C = cC[i], M = cM[i], HH = cH[i], H2u = cH2u[i];
+            if (DIM == 3) {
+                P[i] = P[i] - dt * (C * (uxx + uyy + uzz) + M * (wx + wy + wz));
+                TXX[i] = TXX[i] + dt * (H2u * (uyy + uzz) + HH * uxx + C * (wx + wy + wz));
+                TYY[i] = TYY[i] + dt * (H2u * (uxx + uzz) + HH * uyy + C * (wx + wy + wz));
+                TZZ[i] = TZZ[i] + dt * (H2u * (uxx + uyy) + HH * uzz + C * (wx + wy + wz));
+                TXY[i] = TXY[i] + muxy[i] * dt * (uxy + uyx);
+                TYZ[i] = TYZ[i] + muyz[i] * dt * (uyz + uzy);
+                TXZ[i] = TXZ[i] + muxz[i] * dt * (uxz + uzx);
+            } else {
+                P[i] = P[i] - dt * (C * (uxx + uzz) + M * (wx + wz));
+                TXX[i] = TXX[i] + dt * (H2u * uzz + HH * uxx + C * (wx + wz));
+                TZZ[i] = TZZ[i] + dt * (H2u * uxx + HH * uzz + C * (wx + wz));
+                TXZ[i] = TXZ[i] + muxz[i] * dt * (uxz + uzx);
+            }
+        }
+    }
+
+    template <int DIM, int ORD>
+    void phases() {
+        const int ylo = DIM == 3 ? hw : 0, yhi = DIM == 3 ? ny - hw : 1;
+#pragma omp parallel for schedule(static) collapse(2)
+        for (int z = hw; z < nz - hw; z++)
+            for (int y = ylo; y < yhi; y++) v_row<DIM, ORD>(y, z);
+#pragma omp parallel for schedule(static) collapse(2)
+        for (int z = hw; z < nz - hw; z++)
+            for (int y = ylo; y < yhi; y++) t_row<DIM, ORD>(y, z);
+    }
+
+    void step() {
+        inject();
+        if (dim == 3) { if (order == 2) phases<3, 2>(); else phases<3, 4>(); }
+        else { if (order == 2) phases<2, 2>(); else phases<2, 4>(); }
+        record();
+        it++;
+    }
+
+    void record() {
+        if (it < cfg.nt) {
+            int nr = cfg.nrec;
+            for (int r = 0; r < nr; r++) {
+                size_t i = rec_idx[r];
+                size_t base = (size_t)r * cfg.nt + it;
+                size_t cs = (size_t)nr * cfg.nt;
+                traces[0 * cs + base] = (float)f[BP_F_TXX][i];
+                traces[1 * cs + base] = (float)f[BP_F_TZZ][i];
+                traces[2 * cs + base] = (float)f[BP_F_VUX][i];
+                traces[3 * cs + base] = (float)f[BP_F_VWX][i];
+                traces[4 * cs + base] = (float)f[BP_F_P][i];
+            }
+        }
+        for (size_t k = 0; k < snap_steps.size(); k++) {
+            if (snap_steps[k] != it) continue;
+            for (int fi = 0; fi < BP_NFIELDS; fi++) {
+                if (!(snap_masks[k] & (1u << fi)) || !field_used(fi)) continue;
+                std::vector<float>& out = snaps[k * BP_NFIELDS + fi];
+                out.resize(snap_n);
+                if (snap_n == ncell) {
+                    for (size_t i = 0; i < ncell; i++) out[i] = (float)f[fi][i];
+                } else {
+                    int y = cfg.snap_y;
+                    for (int z = 0; z < nz; z++)
+                        for (int x = 0; x < nx; x++) out[(size_t)z * nx + x] = (float)f[fi][x + y * sy + z * sz];
+                }
+            }
+        }
+    }
+};
+
+struct Handle {
+    int mode;
+    void* impl;
+};
+
+template <typename T, bool REF>
+Oracle<T, REF>* as(Handle* h) { return (Oracle<T, REF>*)h->impl; }
+
+}  // namespace
+
+extern "C" {
+
+// ---- IEEE binary16 round-to-nearest-even conversion (own implementation) ----
+uint16_t orc_f2h(float v) {
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    uint32_t sign = (u >> 16) & 0x8000u;
+    uint32_t ex = (u >> 23) & 0xffu;
+    uint32_t man = u & 0x7fffffu;
+    if (ex == 0xffu) return (uint16_t)(sign | 0x7c00u | (man ? 0x200u : 0u));
+    int e = (int)ex - 127 + 15;
+    if (e >= 31) return (uint16_t)(sign | 0x7c00u);
+    if (e <= 0) {
+        if (e < -10) return (uint16_t)sign;
+        man |= 0x800000u;
+        int shift = 14 - e;  // 24-bit significand -> subnormal half
+        uint32_t q = man >> shift;
+        uint32_t rem = man & ((1u << shift) - 1u);
+        uint32_t half = 1u << (shift - 1);
+        if (rem > half || (rem == half && (q & 1u))) q++;
+        return (uint16_t)(sign | q);
+    }
+    uint32_t q = man >> 13;
+    uint32_t rem = man & 0x1fffu;
+    uint32_t h = sign | ((uint32_t)e << 10) | q;
+    if (rem > 0x1000u || (rem == 0x1000u && (q & 1u))) h++;  // carry may round up into inf
+    return (uint16_t)h;
+}
+
+float orc_h2f(uint16_t h) {
+    uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+    uint32_t ex = (h >> 10) & 0x1fu;
+    uint32_t man = h & 0x3ffu;
+    uint32_t u;
+    if (ex == 0) {
+        if (man == 0) u = sign;
+        else {
+            int e = -1;
+            do { man <<= 1; e++; } while (!(man & 0x400u));
+            man &= 0x3ffu;
+            u = sign | ((uint32_t)(127 - 15 - e) << 23) | (man << 13);
+        }
+    } else if (ex == 31) {
+        u = sign | 0x7f800000u | (man << 13);
+    } else {
+        u = sign | ((ex - 15 + 127) << 23) | (man << 13);
+    }
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// Compensated codec, Half/main.cu:59-100: v ~ hi + lo * u(hi), u = 2^(e-19)
+// (fp16 ulp / 256) with e from frexpf(|hi|); u = 2^-32 when |hi| < 2^-14.
+float orc_residual_unit(float hi) {
+    float a = std::fabs(hi);
+    if (a < 6.103515625e-5f) return 2.3283064365386963e-10f;
+    int e = 0;
+    std::frexp(a, &e);
+    return std::ldexp(1.0f, e - 19);
+}
+float orc_load_ch(uint16_t hi, int8_t lo) {
+    float h = orc_h2f(hi);
+    return h + (float)lo * orc_residual_unit(h);
+}
+void orc_store_ch(float v, uint16_t* hi, int8_t* lo) {
+    uint16_t h = orc_f2h(v);
+    float hf = orc_h2f(h);
+    float scaled = (v - hf) / orc_residual_unit(hf);
+    int q = (int)(scaled + (scaled >= 0.0f ? 0.5f : -0.5f));
+    if (q > 127) q = 127;
+    if (q < -127) q = -127;
+    *hi = h;
+    *lo = (int8_t)q;
+}
+void orc_encode_array(const float* v, size_t n, uint16_t* hi, int8_t* lo) {
+    for (size_t i = 0; i < n; i++) orc_store_ch(v[i], hi + i, lo + i);
+}
+void orc_f2h_array(const float* v, size_t n, uint16_t* out) {
+    for (size_t i = 0; i < n; i++) out[i] = orc_f2h(v[i]);
+}
+
+// create_model (Float/main.cu:1590-1655): borehole of radius^2 <= 100 cells.
+int orc_medium_reference_borehole(int nx, int ny, int nz, float* out9) {
+    size_t n = (size_t)nx * ny * nz;
+    float* rho = out9 + 0 * n; float* rhofo = out9 + 1 * n; float* M = out9 + 2 * n;
+    float* C = out9 + 3 * n; float* HH = out9 + 4 * n; float* H2u = out9 + 5 * n;
+    float* mu = out9 + 6 * n; float* C1 = out9 + 7 * n; float* C2 = out9 + 8 * n;
+    double Ks1, Kb1, Kf1, a1, tao, eta, porousm, perm, por;
+    porousm = 8; eta = 1.0 * pow(10.0, -3);
+    for (int iz = 0; iz < nz; iz++)
+        for (int iy = 0; iy < ny; iy++)
+            for (int ix = 0; ix < nx; ix++) {
+                size_t i = ix + (size_t)iy * nx + (size_t)iz * nx * ny;
+                float vp, vs, vf, rhos, rhof, rhov, muv;
+                if (((ix - nx / 2) * (ix - nx / 2) + (iy - ny / 2) * (iy - ny / 2)) <= 100) {
+                    vp = 1500.0f; vs = 0.0f; vf = 1500.0f; rhos = 1000.0f; rhof = 1000.0f; rhov = 1000.0f;
+                    por = 1.0; muv = 0.0f; Kb1 = 0.0;
+                    Ks1 = rhof * vp * vp;
+                    Kf1 = rhof * vf * vf;
+                    C[i] = Kf1; M[i] = Kf1; HH[i] = Kf1; H2u[i] = Kf1;
+                    C1[i] = 0.0f; C2[i] = rhof;
+                    (void)Ks1; (void)vs; (void)rhos;
+                } else {
+                    vp = 4000.0f; vs = 2700.0f; rhos = 2650.0f; rhof = 1000.0f; vf = 1500.0f;
+                    por = 0.1;
+                    rhov = (1 - por) * rhos + por * rhof;
+                    perm = 2 * pow(10.0, -12);
+                    muv = (1 - por) * rhos * vs * vs;
+                    Kb1 = rhos * (1 - por) * (vp * vp - vs * vs * 4.0 / 3.0);
+                    Ks1 = rhos * (vp * vp - vs * vs * 4.0 / 3.0);
+                    Kf1 = rhof * vf * vf;
+                    tao = 3.0;
+                    a1 = 1 - Kb1 / Ks1;
+                    M[i] = Kf1 * Ks1 / (por * Ks1 + (a1 - por) * Kf1);
+                    HH[i] = a1 * a1 * M[i] + Kb1 + muv * 4.0 / 3.0;
+                    H2u[i] = HH[i] - 2 * muv;
+                    C[i] = M[i] * a1;
+                    C1[i] = eta / perm;
+                    C2[i] = (1 + 2 / porousm) * tao * rhof / por;
+                }
+                rho[i] = rhov; rhofo[i] = rhof; mu[i] = muv;
+            }
+    return 0;
+}
+
+void* orc_create(const bp_config* cfg, const bp_medium* m, int mode) {
+    Handle* h = new Handle();
+    h->mode = mode;
+    if (mode == ORC_REF32) {
+        auto* o = new Oracle<float, true>();
+        o->setup(cfg, m);
+        h->impl = o;
+    } else {
+        auto* o = new Oracle<double, false>();
+        o->setup(cfg, m);
+        h->impl = o;
+    }
+    return h;
+}
+
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+int orc_get_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+// Subnormal floats appear ahead of the wavefront and in the CPML and x86
+// handles them slowly.  Flushing them is available for timing-only runs; it is
+// off by default because the reference's GPU build keeps subnormals and the
+// restatement must match it (flushing moves the step-500 vux slice from 3.5e-6
+// to 1.5e-5 rel-L2 against the reference's golden file).
+static int g_ftz = 0;
+void orc_set_ftz(int on) { g_ftz = on; }
+
+int orc_run(void* hv, int nsteps) {
+    Handle* h = (Handle*)hv;
+    unsigned mode = g_ftz ? (_mm_getcsr() | 0x8040u) : (_mm_getcsr() & ~0x8040u);
+#pragma omp parallel
+    { _mm_setcsr(mode); }
+    _mm_setcsr(mode);
+    for (int s = 0; s < nsteps; s++) {
+        if (h->mode == ORC_REF32) as<float, true>(h)->step();
+        else as<double, false>(h)->step();
+    }
+    return 0;
+}
+
+#define ORC_DISPATCH(h, ...)                            \
+    do {                                                \
+        if ((h)->mode == ORC_REF32) {                   \
+            auto* o = as<float, true>(h); __VA_ARGS__;  \
+        } else {                                        \
+            auto* o = as<double, false>(h); __VA_ARGS__; \
+        }                                               \
+    } while (0)
+
+int orc_get_traces(void* hv, int comp, float* out, size_t n) {
+    Handle* h = (Handle*)hv;
+    int rc = 0;
+    ORC_DISPATCH(h, {
+        size_t cs = (size_t)o->cfg.nrec * o->cfg.nt;
+        if (comp < 0 || comp >= BP_NTRACE || n < cs) rc = BP_ERR_ARG;
+        else std::memcpy(out, o->traces.data() + comp * cs, cs * sizeof(float));
+    });
+    return rc;
+}
+
+int orc_get_field(void* hv, int field, double* out, size_t n) {
+    Handle* h = (Handle*)hv;
+    int rc = 0;
+    ORC_DISPATCH(h, {
+        if (field < 0 || field >= BP_NFIELDS || n < o->ncell || o->f[field].empty()) rc = BP_ERR_ARG;
+        else for (size_t i = 0; i < o->ncell; i++) out[i] = (double)o->f[field][i];
+    });
+    return rc;
+}
+
+int orc_get_snapshot(void* hv, int k, int field, float* out, size_t n) {
+    Handle* h = (Handle*)hv;
+    int rc = 0;
+    ORC_DISPATCH(h, {
+        if (k < 0 || k >= (int)o->snap_steps.size() || field < 0 || field >= BP_NFIELDS) rc = BP_ERR_ARG;
+        else {
+            const std::vector<float>& s = o->snaps[(size_t)k * BP_NFIELDS + field];
+            if (s.empty()) rc = BP_ERR_NOT_FOUND;
+            else if (n < s.size()) rc = BP_ERR_ARG;
+            else std::memcpy(out, s.data(), s.size() * sizeof(float));
+        }
+    });
+    return rc;
+}
+
+// Coefficient arrays by name (full padded grid) for precompute parity tests.
+int orc_get_coef(void* hv, const char* name, double* out, size_t n) {
+    Handle* h = (Handle*)hv;
+    int rc = 0;
+    ORC_DISPATCH(h, {
+        const char* names[] = {"rhox", "rhoy", "rhoz", "rhof", "C1x", "C1y", "C1z", "C2x", "C2y", "C2z",
+                               "C", "M", "H", "H2u", "muxy", "muxz", "muyz"};
+        decltype(&o->rhox) arr[] = {&o->rhox, &o->rhoy, &o->rhoz, &o->rhof, &o->C1x, &o->C1y, &o->C1z,
+                                    &o->C2x, &o->C2y, &o->C2z, &o->cC, &o->cM, &o->cH, &o->cH2u,
+                                    &o->muxy, &o->muxz, &o->muyz};
+        rc = BP_ERR_NOT_FOUND;
+        for (int k = 0; k < 17; k++)
+            if (!std::strcmp(name, names[k])) {
+                if (arr[k]->empty()) { rc = BP_ERR_NOT_FOUND; break; }
+                if (n < o->ncell) { rc = BP_ERR_ARG; break; }
+                for (size_t i = 0; i < o->ncell; i++) out[i] = (double)(*arr[k])[i];
+                rc = 0;
+                break;
+            }
+    });
+    return rc;
+}
+
+// Profile table of one axis: which 0 = d, 1 = e, 2 = d2, 3 = e2 (float tables),
+// 4..7 the same in FP64.
+int orc_get_profile(void* hv, int axis, int which, double* out, size_t n) {
+    Handle* h = (Handle*)hv;
+    int rc = 0;
+    ORC_DISPATCH(h, {
+        const Profile& p = o->prof[axis];
+        size_t len = p.d.size();
+        if (len == 0 || n < len || which < 0 || which > 7) rc = BP_ERR_ARG;
+        else for (size_t i = 0; i < len; i++) {
+            switch (which) {
+                case 0: out[i] = p.d[i]; break;
+                case 1: out[i] = p.e[i]; break;
+                case 2: out[i] = p.d2[i]; break;
+                case 3: out[i] = p.e2[i]; break;
+                case 4: out[i] = p.dd[i]; break;
+                case 5: out[i] = p.ed[i]; break;
+                case 6: out[i] = p.dd2[i]; break;
+                default: out[i] = p.ed2[i]; break;
+            }
+        }
+    });
+    return rc;
+}
+
+int orc_get_step(void* hv) {
+    Handle* h = (Handle*)hv;
+    int s = 0;
+    ORC_DISPATCH(h, { s = o->it; });
+    return s;
+}
+
+float orc_ricker_ref(int it, float DT, float F0, float T0) { return ricker_ref(it, DT, F0, T0); }
+
+// Exponent scaling of Half/main.cu:745-843 restated over the reference-shaped
+// float coefficient arrays of a REF32 oracle: K_max over |H|,|H-2mu|,|C|,|M|,
+// |mu| and the staggered mu; R_max over rho^-1 > 0 and, where C1 != 0 and
+// |Q| > 1e-12, 1/|Q| and |rhof rho^-1 / Q|.  Returns e_m, e_pml.
+int orc_comp16_exponents(void* hv, const float* mu_cell_padded, int* em, int* epml,
+                         float* kmax_out, float* rmax_out) {
+    Handle* h = (Handle*)hv;
+    if (h->mode != ORC_REF32) return BP_ERR_ARG;
+    auto* o = as<float, true>(h);
+    float Kmax = 0.0f, Rmax = 0.0f;
+    const float Q_EPS = 1.0e-12f;
+    float DT = o->DT;
+    for (size_t i = 0; i < o->ncell; i++) {
+        Kmax = fmaxf(Kmax, fabsf(o->cH[i]));
+        Kmax = fmaxf(Kmax, fabsf(o->cH2u[i]));
+        Kmax = fmaxf(Kmax, fabsf(o->cC[i]));
+        Kmax = fmaxf(Kmax, fabsf(o->cM[i]));
+        if (mu_cell_padded) Kmax = fmaxf(Kmax, fabsf(mu_cell_padded[i]));
+        Kmax = fmaxf(Kmax, fabsf(o->muxz[i]));
+        if (o->dim == 3) {
+            Kmax = fmaxf(Kmax, fabsf(o->muxy[i]));
+            Kmax = fmaxf(Kmax, fabsf(o->muyz[i]));
+        }
+        float rhof0 = o->rhof[i];
+        const std::vector<float>* R[3] = {&o->rhox, o->dim == 3 ? &o->rhoy : nullptr, &o->rhoz};
+        const std::vector<float>* C1[3] = {&o->C1x, o->dim == 3 ? &o->C1y : nullptr, &o->C1z};
+        const std::vector<float>* C2[3] = {&o->C2x, o->dim == 3 ? &o->C2y : nullptr, &o->C2z};
+        for (int a = 0; a < 3; a++) {
+            if (!R[a]) continue;
+            float ri = (*R[a])[i];
+            if (ri > 0.0f) Rmax = fmaxf(Rmax, fabsf(ri));
+            float Q = (*C2[a])[i] - rhof0 * rhof0 * ri;
+            if ((*C1[a])[i] != 0.0f && fabsf(Q) > Q_EPS) {
+                Rmax = fmaxf(Rmax, 1.0f / fabsf(Q));
+                Rmax = fmaxf(Rmax, fabsf(rhof0 * ri / Q));
+            }
+        }
+    }
+    int e_m = -23;
+    if (Kmax > 0.0f && Rmax > 0.0f) {
+        float er = 1.0f / sqrtf(DT * DT * Kmax * Rmax);
+        e_m = (int)lrintf(-log2f(er * DT * Kmax));
+    }
+    float pml_max = 0.0f;
+    for (int a = 0; a < 3; a++) {
+        const Profile& p = o->prof[a];
+        for (size_t i = 0; i < p.d.size(); i++) {
+            pml_max = fmaxf(pml_max, fabsf(DT * p.d[i]));
+            pml_max = fmaxf(pml_max, fabsf(DT * p.d2[i]));
+            pml_max = fmaxf(pml_max, fabsf(1.0f - p.e[i]));
+            pml_max = fmaxf(pml_max, fabsf(1.0f - p.e2[i]));
+        }
+    }
+    int e_pml = 0;
+    if (pml_max > 0.0f) {
+        e_pml = (int)floorf(log2f(2048.0f / pml_max));
+        if (e_pml > 20) e_pml = 20;
+        if (e_pml < -20) e_pml = -20;
+    }
+    *em = e_m; *epml = e_pml;
+    if (kmax_out) *kmax_out = Kmax;
+    if (rmax_out) *rmax_out = Rmax;
+    return 0;
+}
+
+void orc_destroy(void* hv) {
+    Handle* h = (Handle*)hv;
+    if (!h) return;
+    if (h->mode == ORC_REF32) delete as<float, true>(h);
+    else delete as<double, false>(h);
+    delete h;
+}
+
+}  // extern "C"

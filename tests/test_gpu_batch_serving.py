@@ -1,0 +1,87 @@
+"""Batched shots and the serving loop.
+
+A shot's arithmetic depends only on its own arrays, so its traces are
+bit-identical alone, in a batch, and in a server mix (the tolerance is 0).
+"""
+import time
+
+import numpy as np
+import pytest
+
+from mixedprecisionfaracoustic_b200 import Batch, Server, Simulation
+from mixedprecisionfaracoustic_b200.presets import config3_shots, config4_requests
+
+pytestmark = pytest.mark.gpu
+
+
+def alone(cfg, med):
+    with Simulation(cfg, med) as s:
+        s.run(cfg.nt)
+        return s.traces("txx"), s.traces("p")
+
+
+@pytest.mark.parametrize("prec", ["fp32", "comp16"])
+def test_batch_equals_single_shots(prec):
+    shots = config3_shots(seed=3, nshots=5, nt=160, precision=prec, scale=0.08)
+    b = Batch([c for c, _ in shots], [m for _, m in shots])
+    b.run(160)
+    b.sync()
+    for i, (cfg, med) in enumerate(shots):
+        tx, tp = alone(cfg, med)
+        assert np.array_equal(b.traces(i, "txx"), tx), i
+        assert np.array_equal(b.traces(i, "p"), tp), i
+    t = b.tune()
+    assert t["steps_per_sync"] > 0 and t["tile_rows"] > 0
+    assert b.cell_updates() == sum(c.nt * (c.nx + 2 * c.npml - 2) * (c.nz + 2 * c.npml - 2) for c, _ in shots)
+    b.close()
+
+
+def test_batch_shots_with_different_lengths():
+    shots = config3_shots(seed=5, nshots=3, nt=100, precision="fp32", scale=0.06)
+    shots[1][0].nt = 40
+    shots[2][0].nt = 130
+    b = Batch([c for c, _ in shots], [m for _, m in shots], steps_per_sync=16, ctas_per_sm=2)
+    b.run(200)
+    for i, (cfg, med) in enumerate(shots):
+        tx, _ = alone(cfg, med)
+        assert np.array_equal(b.traces(i, "txx"), tx), i
+    b.close()
+
+
+def test_server_invariance_and_admission():
+    reqs = config4_requests(seed=4, n=8, precision="fp32", scale=0.05, steps=(60, 200), include_3d=True)
+    singles = [alone(c, m)[0] for c, m in reqs]
+    # budget that fits only a few shots at once: forces queueing + continuous batching
+    from mixedprecisionfaracoustic_b200 import _abi
+    import ctypes as C
+    sizes = []
+    for c, _ in reqs:
+        b = C.c_size_t()
+        sizes.append(c)
+    srv = Server(hbm_budget_bytes=256 << 20, steps_per_sync=20)
+    ids = []
+    for c, m in reqs:
+        ids.append(srv.submit(c, m))
+        time.sleep(0.01)
+    for rid in ids:
+        srv.wait(rid, 300)
+    for rid, ref in zip(ids, singles):
+        assert srv.poll(rid) == "done"
+        assert np.array_equal(srv.traces(rid, "txx"), ref)
+        assert srv.latency(rid) > 0
+    st = srv.stats()
+    assert st["completed"] == len(reqs)
+    assert st["p99_latency_s"] >= st["p50_latency_s"] > 0
+    assert st["max_resident"] >= 2
+    assert st["hbm_in_use"] == 0
+    srv.close()
+
+
+def test_server_rejects_oversized_request():
+    (c, m), = config4_requests(seed=9, n=1, scale=0.05, steps=(50, 60), include_3d=False)
+    srv = Server(hbm_budget_bytes=1 << 20, steps_per_sync=10)
+    from mixedprecisionfaracoustic_b200._abi import BiotError, BP_ERR_BUDGET
+    with pytest.raises(BiotError) as e:
+        srv.submit(c, m)
+    assert e.value.code == BP_ERR_BUDGET
+    srv.close()

@@ -1,0 +1,166 @@
+"""CUDA path vs the CPU oracle on the same seeded inputs (small grids).
+
+Tolerances (relative L2 over all receivers and steps, or over the field):
+  FP32   vs oracle REF32 (the Float build's arithmetic)   <= 1e-5
+  FP64   vs oracle FP64                                     <= 1e-10
+  COMP16 vs oracle FP64                                     <= 1e-3
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from mixedprecisionfaracoustic_b200 import Simulation
+from mixedprecisionfaracoustic_b200 import _abi
+from mixedprecisionfaracoustic_b200.biot import Medium, ShotConfig
+from mixedprecisionfaracoustic_b200.presets import config0, config1, layered_medium
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def small_3d(order=2, precision="fp32", n=24, npml=8, nt=120, borehole=True):
+    """Reference-style 3D case: borehole medium, CPML on all faces, 3 kHz source."""
+    nxe = n + 2 * npml
+    med = Medium.from_stack(O.borehole_medium(n, n, n), (n, n, n))
+    c = nxe // 2
+    cfg = ShotConfig(dim=3, nx=n, ny=n, nz=n, npml=npml, order=order, precision=precision, nt=nt,
+                     dx=0.01, dt=0.9e-6, f0=3000.0, t0=float(np.float32(1.2 / 3000.0)), pml_v0=4000.0, pml_r=1e-6,
+                     src=(c, c, npml + 3), src_mask=_abi.SRC_TAU,
+                     rec_x=[c] * nxe + list(range(nxe)), rec_y=[c] * (2 * nxe),
+                     rec_z=list(range(nxe)) + [c + 2] * nxe,
+                     snap_steps=[nt // 2], snap_fields=["txx", "vux", "vwz", "p"], snap_y=c + 1)
+    return cfg, med
+
+
+def small_2d(order=2, precision="fp32", nx=96, nz=64, npml=10, nt=300):
+    cfg, med = config1(precision=precision, nx=nx, nz=nz, nt=nt, npml=npml, order=order, nrec=48)
+    cfg.check_cfl = 1
+    return cfg, med
+
+
+def run_gpu(cfg, med):
+    with Simulation(cfg, med) as s:
+        s.run(cfg.nt)
+        tr = {c: s.traces(c) for c in _abi.TRACES}
+        fl = {f: s.field(f) for f in ("vux", "vuz", "vwx", "vwz", "p", "txx", "tzz", "txz")}
+        return tr, fl
+
+
+def run_oracle(cfg, med, mode):
+    o = O.Oracle(cfg, med, mode)
+    o.run(cfg.nt)
+    tr = {c: o.traces(c) for c in _abi.TRACES}
+    fl = {f: o.field(f) for f in ("vux", "vuz", "vwx", "vwz", "p", "txx", "tzz", "txz")}
+    return tr, fl
+
+
+CASES = [("3d", 2), ("3d", 4), ("2d", 2), ("2d", 4)]
+
+
+def make(kind, order, precision):
+    return small_3d(order, precision) if kind == "3d" else small_2d(order, precision)
+
+
+@pytest.mark.parametrize("kind,order", CASES)
+def test_fp32_matches_oracle_ref32(kind, order):
+    cfg, med = make(kind, order, "fp32")
+    gt, gf = run_gpu(cfg, med)
+    ot, of = run_oracle(cfg, med, O.REF32)
+    for c in _abi.TRACES:
+        assert np.abs(ot[c]).max() > 0
+        assert rel_l2(gt[c], ot[c]) <= 1e-5, (c, rel_l2(gt[c], ot[c]))
+    for f in gf:
+        assert rel_l2(gf[f], of[f]) <= 1e-5, (f, rel_l2(gf[f], of[f]))
+
+
+@pytest.mark.parametrize("kind,order", CASES)
+def test_fp64_matches_oracle_fp64(kind, order):
+    cfg, med = make(kind, order, "fp64")
+    gt, gf = run_gpu(cfg, med)
+    ot, of = run_oracle(cfg, med, O.FP64)
+    for f in gf:
+        assert rel_l2(gf[f], of[f]) <= 1e-10, (f, rel_l2(gf[f], of[f]))
+
+
+@pytest.mark.parametrize("kind,order", CASES)
+def test_comp16_within_1e3_of_fp64(kind, order):
+    cfg, med = make(kind, order, "comp16")
+    gt, gf = run_gpu(cfg, med)
+    ot, of = run_oracle(cfg, med, O.FP64)
+    for c in ("txx", "tzz", "vux", "p"):
+        assert rel_l2(gt[c], ot[c]) <= 1e-3, (c, rel_l2(gt[c], ot[c]))
+
+
+def test_snapshots_match_oracle():
+    cfg, med = small_3d(2, "fp32")
+    with Simulation(cfg, med) as s:
+        s.run(cfg.nt)
+        g = {f: s.snapshot(0, f) for f in ("txx", "vux", "vwz", "p")}
+    o = O.Oracle(cfg, med, O.REF32)
+    o.run(cfg.nt)
+    for f, a in g.items():
+        b = o.snapshot(0, f)
+        assert a.shape == b.shape
+        assert rel_l2(a, b) <= 1e-5, f
+
+
+@pytest.mark.parametrize("prec,mode", [("fp32", O.REF32), ("fp64", O.FP64)])
+def test_coefficients_match_oracle(prec, mode):
+    """GPU FP64 precompute vs the oracle's restatement of Float/main.cu:472-513."""
+    cfg, med = small_3d(2, prec, nt=4)
+    with Simulation(cfg, med) as s:
+        g = {n: s.coef(n) for n in ("rho_x", "rho_y", "rho_z", "rhof", "C", "M", "H", "H2u",
+                                    "mu_xy", "mu_xz", "mu_yz")}
+    o = O.Oracle(cfg, med, mode)
+    names = {"rho_x": "rhox", "rho_y": "rhoy", "rho_z": "rhoz", "rhof": "rhof", "C": "C", "M": "M", "H": "H",
+             "H2u": "H2u", "mu_xy": "muxy", "mu_xz": "muxz", "mu_yz": "muyz"}
+    sl = (slice(1, -1),) * 3
+    for n, on in names.items():
+        a, b = g[n][sl].astype(np.float64), o.coef(on)[sl]
+        tol = 3e-7 if prec == "fp32" else 1e-7
+        assert np.allclose(a, b, rtol=tol, atol=0), (n, np.abs(a - b).max())
+
+
+def test_energy_matches_oracle_fields():
+    cfg, med = small_2d(2, "fp64", nt=150)
+    with Simulation(cfg, med) as s:
+        s.run(cfg.nt)
+        e = s.energy()
+    o = O.Oracle(cfg, med, O.FP64)
+    o.run(cfg.nt)
+    ref = sum(float((o.field(f) ** 2).sum()) for f in ("vux", "vuz", "vwx", "vwz", "p", "txx", "tzz", "txz"))
+    assert abs(e - ref) <= 1e-9 * ref
+
+
+def test_rel_l2_device_matches_numpy():
+    import torch
+    x = torch.randn(1 << 20, device="cuda", dtype=torch.float32)
+    r = torch.randn(1 << 20, device="cuda", dtype=torch.float32)
+    import ctypes as C
+    v = C.c_double()
+    lib = _abi.load()
+    _abi.check(lib.bp_rel_l2_device(C.c_void_p(x.data_ptr()), C.c_void_p(r.data_ptr()), x.numel(), C.byref(v)),
+               "bp_rel_l2_device")
+    ref = rel_l2(x.cpu().numpy(), r.cpu().numpy())
+    assert abs(v.value - ref) <= 1e-9 * ref
+
+
+def test_run_in_chunks_equals_one_run():
+    """Graph replays, direct chunks and snapshot splits give bit-identical results."""
+    cfg, med = small_2d(2, "fp32", nt=170)
+    with Simulation(cfg, med) as a:
+        a.run(cfg.nt)
+        ta = a.traces("txx")
+    with Simulation(cfg, med) as b:
+        for n in (1, 7, 32, 64, 3, 100):
+            b.run(n)
+        tb = b.traces("txx")
+    assert np.array_equal(ta, tb)
+
+
+def test_c0_order4_3d_fp32_vs_oracle():
+    cfg, med = config0(precision="fp32", order=4, n=40, npml=10, nt=120, nrec=32)
+    gt, gf = run_gpu(cfg, med)
+    ot, of = run_oracle(cfg, med, O.REF32)
+    for c in _abi.TRACES:
+        assert rel_l2(gt[c], ot[c]) <= 1e-5, c

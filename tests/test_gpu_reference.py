@@ -1,0 +1,68 @@
+"""The drop-in run: the reference program's configuration on the GPU.
+
+Checks the FP32 path against the reference's own golden slices (state after
+step 500, Float/*.dat) and the text files the drop-in writes against the
+reference's format (wfile / wfile3d, Float/main.cu:1501-1516,1563-1588).
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from mixedprecisionfaracoustic_b200 import Simulation
+from mixedprecisionfaracoustic_b200.presets import reference_compat
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ref_run(tmp_path_factory):
+    cfg, med = reference_compat(nt=501)
+    s = Simulation(cfg, med)
+    s.run(501)
+    out = tmp_path_factory.mktemp("refout")
+    s.write_reference_outputs(out)
+    yield s, out
+    s.close()
+
+
+@pytest.mark.parametrize("field", ["txx", "vux", "vuz", "vwx", "vwz"])
+def test_fp32_matches_reference_golden(ref_run, golden, field):
+    s, _ = ref_run
+    a = s.snapshot(0, field)
+    assert a.shape == (192, 192)
+    err = rel_l2(a, golden[field + "500"])
+    assert err <= 1e-5, f"{field}500 rel L2 {err:.3e}"
+
+
+def _parse(path):
+    return np.array([[float(v) for v in ln.split()] for ln in path.read_text().splitlines() if ln.strip()])
+
+
+def test_reference_text_format(ref_run, golden):
+    _, out = ref_run
+    names = sorted(p.name for p in out.iterdir())
+    for n in ["sisx.dat", "sisz.dat", "sisvu.dat", "sisvw.dat", "sisp.dat", "txx500.dat", "vux500.dat",
+              "vwx500.dat", "vuz500.dat", "vwz500.dat", "txx.dat"]:
+        assert n in names, n
+    raw = (out / "txx500.dat").read_text()
+    rows = raw.split("\n")
+    # 192 rows of 192 "%e " values, each row terminated by "\n\n"
+    assert raw.count("\n") == 2 * 192
+    assert rows[0].endswith(" ") and len(rows[0].split()) == 192 and rows[1] == ""
+    a = _parse(out / "txx500.dat")
+    assert a.shape == (192, 192)
+    assert rel_l2(a, golden["txx500"]) <= 1e-5
+    sis = _parse(out / "sisx.dat")
+    assert sis.shape == (192, 501)
+
+
+def test_comp16_reference_run_vs_fp64():
+    cfg, med = reference_compat(nt=301, precision="comp16")
+    c64, _ = reference_compat(nt=301, precision="fp64")
+    with Simulation(cfg, med) as a, Simulation(c64, med) as b:
+        a.run(301)
+        b.run(301)
+        for c in ("txx", "tzz", "vux", "p"):
+            assert a.trace_rel_l2(b, c) <= 1e-3, c
+        sc = a.scaling()
+    assert sc["em"] == -23          # method.md worked example for this medium

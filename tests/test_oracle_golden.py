@@ -1,0 +1,41 @@
+"""Pins the CPU oracle to the reference's own output.
+
+The reference ships the y-mid slices of its Float run (Float/txx500.dat,
+vux500.dat, vuz500.dat, vwx500.dat, vwz500.dat: state after step it = 500,
+Float/main.cu:1094-1108,1191-1211).  The oracle's restatement of the Float
+arithmetic (REF32) must reproduce them to the precision of the "%e" text
+format plus FMA-contraction differences: relative L2 <= 1e-5 per field.
+This runs the full 192^3 grid for 501 steps on the CPU (~2-3 minutes).
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from mixedprecisionfaracoustic_b200.biot import Medium
+from mixedprecisionfaracoustic_b200.presets import reference_compat_config
+from oracle import oracle as O
+
+
+@pytest.fixture(scope="module")
+def ref32_step500():
+    cfg = reference_compat_config(nt=600)
+    med = Medium.from_stack(O.borehole_medium(128, 128, 128), (128, 128, 128))
+    o = O.Oracle(cfg, med, O.REF32)
+    o.run(501)
+    return o
+
+
+@pytest.mark.parametrize("field", ["txx", "vux", "vuz", "vwx", "vwz"])
+def test_oracle_matches_reference_golden(ref32_step500, golden, field):
+    a = ref32_step500.snapshot(0, field)
+    b = golden[field + "500"]
+    assert a.shape == (192, 192)
+    err = rel_l2(a, b)
+    assert err <= 1e-5, f"{field}500: rel L2 {err:.3e}"
+
+
+def test_golden_source_cell(golden):
+    # the shipped slice peaks at the source cell (iz = 20 + NP = 52, ix = 96)
+    t = golden["txx500"]
+    iz, ix = np.unravel_index(np.argmax(np.abs(t)), t.shape)
+    assert (iz, ix) == (52, 96)
