@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--nz", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=20)
+    ap.add_argument("--only", choices=["fp32", "comp16"], default=None,
+                    help="time one precision only and skip the FP64, e2e and CPU legs (profiling runs)")
     return ap.parse_args()
 
 
@@ -149,7 +151,8 @@ def run_ours(args, rank, ws):
     peak, peak_kind = measured_peaks()
     res = {}
     sims = {}
-    for prec in ("fp32", "comp16"):
+    precs = (args.only,) if args.only else ("fp32", "comp16")
+    for prec in precs:
         cfg, med = workload(prec, nt, args.nx, args.nz)
         cfg.device = dev
         s = Simulation(cfg, med)
@@ -184,6 +187,10 @@ def run_ours(args, rank, ws):
             "cells": cells,
         }
         sims[prec] = s
+    if args.only:
+        for s in sims.values():
+            s.close()
+        return res, None
     # FP64 run of the same steps: seismogram relative L2 of both paths
     cfg, med = workload("fp64", nt, args.nx, args.nz)
     cfg.device = dev
@@ -230,22 +237,25 @@ def cpu_baseline(args, budget_s=20.0):
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     O.set_threads(threads)
-    nz = args.nz
-    cfg, med = workload("fp32", 64, args.nx, nz)
-    o = O.Oracle(cfg, med, O.REF32)
-    o.run(1)
+    cfg, med = workload("fp32", 8, args.nx, args.nz)
+    probe = O.Oracle(cfg, med, O.REF32)
+    probe.run(2)
     t0 = time.perf_counter()
+    probe.run(3)
+    per = (time.perf_counter() - t0) / 3
+    probe.close()
+    n = int(max(3, budget_s / max(per, 1e-6)))
+    cfg, med = workload("fp32", n + 4, args.nx, args.nz)
+    o = O.Oracle(cfg, med, O.REF32)
     o.run(2)
-    per = (time.perf_counter() - t0) / 2
-    n = int(max(2, min(60, budget_s / max(per, 1e-6))))
-    n = min(n, cfg.nt - 3)
     t0 = time.perf_counter()
     o.run(n)
     el = time.perf_counter() - t0
     cells = (cfg.padded[0] - 2) * (cfg.padded[2] - 2)
     o.close()
     return {"value": cells * n / el / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": f"c1 full {cfg.padded[0]}x{cfg.padded[2]} grid, steps 3..{3 + n} ({el:.1f} s), REF32 arithmetic"}
+            "sample": f"c1 full {cfg.padded[0]}x{cfg.padded[2]} grid, steps 2..{2 + n} ({el:.1f} s), REF32 arithmetic, "
+                      f"{threads} OpenMP threads"}
 
 
 def run_reference(args, rank, ws):
@@ -300,7 +310,9 @@ def main():
         return 0
     res, e2e = run_ours(args, rank, ws)
     out = None
-    if rank == 0:
+    if args.only and rank == 0:
+        print(json.dumps({"metric": METRIC, "only": args.only, **res[args.only]}), flush=True)
+    elif rank == 0:
         f32, c16 = res["fp32"], res["comp16"]
         cpu = None if (args.no_cpu_baseline or ws > 1) else cpu_baseline(args)
         traffic = ncu_traffic()

@@ -212,6 +212,13 @@ int bp_launches_per_step(bp_sim* sim, int* n);
  * every kernel node they contain). */
 int bp_launch_count(bp_sim* sim, long long* n);
 
+/* The COMP16 storage codec on the device, over host arrays of n values: the
+ * reference's store_ch / load_ch (Half/main.cu:75-100): hi = fp16 RNE(v),
+ * lo = int8 residual in units of fp16-ulp(hi)/256 (2^-32 below 2^-14),
+ * rounded half away from zero and clamped to +-127; v ~ hi + lo * unit. */
+int bp_comp16_encode(const float* host, size_t n, uint16_t* hi, int8_t* lo);
+int bp_comp16_decode(const uint16_t* hi, const int8_t* lo, size_t n, float* out);
+
 /* Relative L2 difference ||x - ref|| / ||ref|| of two DEVICE float arrays of
  * n elements, accumulated in FP64 with warp-shuffle reductions.  Allocates
  * its reduction scratch on the device for the duration of the call. */
@@ -287,6 +294,10 @@ typedef struct bp_server_stats {
     size_t hbm_budget;
     int max_resident;           /* largest number of shots resident at once  */
 } bp_server_stats;
+
+/* Device bytes a shot with this configuration occupies while resident (its
+ * arena plus the transient medium upload): the cost admission charges. */
+int bp_shot_bytes(const bp_config* cfg, size_t* bytes);
 
 /* hbm_budget: bytes of device memory shot state may occupy.
  * steps_per_sync: steps between admission points (0 = 100). */

@@ -85,6 +85,8 @@ _SIGS = [
     ("bp_algorithmic_bytes", C.c_int, [C.c_void_p, DoubleP, C.POINTER(C.c_longlong)]),
     ("bp_launches_per_step", C.c_int, [C.c_void_p, IntP]),
     ("bp_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    ("bp_comp16_encode", C.c_int, [FloatP, C.c_size_t, C.POINTER(C.c_uint16), C.POINTER(C.c_int8)]),
+    ("bp_comp16_decode", C.c_int, [C.POINTER(C.c_uint16), C.POINTER(C.c_int8), C.c_size_t, FloatP]),
     ("bp_rel_l2_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, DoubleP]),
     ("bp_trace_rel_l2", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, DoubleP]),
     ("bp_destroy", None, [C.c_void_p]),
@@ -101,6 +103,7 @@ _SIGS = [
     ("bp_batch_get_tune", C.c_int, [C.c_void_p, C.POINTER(BpTune)]),
     ("bp_batch_cell_updates", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     ("bp_batch_destroy", None, [C.c_void_p]),
+    ("bp_shot_bytes", C.c_int, [C.POINTER(BpConfig), C.POINTER(C.c_size_t)]),
     ("bp_server_create", C.c_int, [C.c_int, C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]),
     ("bp_server_submit", C.c_int, [C.c_void_p, C.POINTER(BpConfig), C.POINTER(BpMedium),
                                    C.POINTER(C.c_uint64)]),

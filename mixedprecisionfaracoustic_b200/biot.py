@@ -132,6 +132,15 @@ def biot_from_moduli(Ks, Kb, mu, Kf, rhos, rhof, phi, tort, eta, kappa, m_shape=
     return dict(zip(MEDIUM_KEYS, list(out)))
 
 
+def shot_bytes(cfg: ShotConfig) -> int:
+    """Device bytes the shot occupies while resident (what serving admission charges)."""
+    lib = load()
+    c = cfg.to_c()
+    n = C.c_size_t()
+    check(lib.bp_shot_bytes(C.byref(c), C.byref(n)), "bp_shot_bytes")
+    return n.value
+
+
 def cfl_limit(cfg: ShotConfig, medium: Medium) -> tuple:
     lib = load()
     c, m = cfg.to_c(), medium.to_c()

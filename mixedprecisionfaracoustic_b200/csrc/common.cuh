@@ -87,6 +87,8 @@ struct ShotDesc {
     int* step_base;               // device: step index `it` of step k=0 of the current chunk
     const float* rtab;            // COMP16: per-step factor applied to old state (dyn[it]/dyn[it-1])
     int src_rec;                  // receiver index that owns the source cell, or -1
+    long long tile0s;             // first tile of this shot in the TMA-staged 2D tiling
+    int nseg_s;                   // 256-cell segments per row in that tiling
     template <class R>
     __device__ __forceinline__ R dtr() const { return sizeof(R) == 8 ? (R)dtd : (R)dt; }
 };
@@ -107,15 +109,36 @@ __device__ __forceinline__ float residual_unit(float hi) {
     int e = (int)((u >> 23) & 0xff) - 126;   // frexpf exponent: a = m * 2^e, m in [0.5,1)
     return __uint_as_float((unsigned)(e - 19 + 127) << 23);
 }
+// The same unit from the fp16 bits: for biased exponent E of hi, frexp gives
+// e = E - 14 (normal) and |hi| < 2^-14 exactly when E <= 1 with 2^(1-33) =
+// 2^-32, so u = 2^(max(E, 1) - 33): float bits (max(E, 1) + 94) << 23.
+__device__ __forceinline__ float unit_from_half_bits(unsigned hb) {
+    unsigned E = (hb >> 10) & 31u;
+    E = E > 1u ? E : 1u;
+    return __uint_as_float((E + 94u) << 23);
+}
+__device__ __forceinline__ float unit_inv_from_half_bits(unsigned hb) {
+    unsigned E = (hb >> 10) & 31u;
+    E = E > 1u ? E : 1u;
+    return __uint_as_float((160u - E) << 23);
+}
 __device__ __forceinline__ float decode_ch(__half hi, int8_t lo) {
-    float h = __half2float(hi);
-    return h + (float)lo * residual_unit(h);
+    return __half2float(hi) + (float)lo * unit_from_half_bits(__half_as_ushort(hi));
+}
+// 1 / residual_unit(hi), also an exact power of two, so the quotient of the
+// reference's (v - hi) / u is formed exactly by a multiplication.
+__device__ __forceinline__ float residual_unit_inv(float hi) {
+    float a = fabsf(hi);
+    if (a < 6.103515625e-5f) return 4294967296.0f;
+    unsigned u = __float_as_uint(a);
+    int e = (int)((u >> 23) & 0xff) - 126;
+    return __uint_as_float((unsigned)(19 - e + 127) << 23);
 }
 __device__ __forceinline__ void encode_ch(float v, __half& hi, int8_t& lo) {
     __half h = __float2half_rn(v);
     float hf = __half2float(h);
-    float scaled = (v - hf) / residual_unit(hf);
-    int q = (int)(scaled + (scaled >= 0.0f ? 0.5f : -0.5f));
+    float scaled = (v - hf) * unit_inv_from_half_bits(__half_as_ushort(h));
+    int q = __float2int_rz(scaled + copysignf(0.5f, scaled));   // round half away from zero
     q = q > 127 ? 127 : (q < -127 ? -127 : q);
     hi = h;
     lo = (int8_t)q;
@@ -206,4 +229,9 @@ struct PolC16 {
     }
 };
 
+}  // namespace bpk
+
+namespace bpk {
+static_assert(sizeof(ShotDesc) % 8 == 0, "ShotDesc is copied to shared memory in 8-byte words");
+static_assert(alignof(ShotDesc) == 8, "ShotDesc alignment");
 }  // namespace bpk

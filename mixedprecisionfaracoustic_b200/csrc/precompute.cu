@@ -274,7 +274,7 @@ __global__ void k_profile(PmlGeom g, double dt, double v0, double rc, R* b, R* e
     const double DP = DPf, H = g.H;
     const double oleft = DPf;
     const double oright = (double)__fsub_rn(__fmul_rn((float)(g.n - 1), g.H), DPf);
-    const double x = (double)__fmul_rn((float)i, g.H);
+    const double x = (double)i * H;     // exact cell position; only the region test uses float x
     const double d0 = 3.0 * v0 * log(1.0 / rc) / (2.0 * DP);
     double d = 0.0, d2 = 0.0;
     if (left) {

@@ -1,5 +1,8 @@
 // runner.h - issues chunks of time steps for a set of shot descriptors, either
 // as direct launches or by replaying a captured CUDA graph of S steps.
+//
+// 2D FP32/COMP16 phases run the TMA-staged kernels (step_staged.cu, one
+// persistent CTA per SM); 3D and FP64 phases the register kernels (step.cu).
 #pragma once
 #include "shot.h"
 
@@ -9,20 +12,22 @@ struct Runner {
     int prec = 0, dim = 2, order = 2;
     const ShotDesc* d_shots = nullptr;
     int nshots = 0;
-    long long ntiles = 0;
+    long long ntiles = 0, ntiles_s = 0;
     int max_rec = 0;
-    int grid_v = 1, grid_t = 1;
+    int grid_v = 1, grid_t = 1, grid_s = 1;
+    bool staged = false;
     cudaStream_t st = nullptr;
     int graph_steps = 0;               // S; 0 disables graphs
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool graph_failed = false;
     long long launches = 0;            // kernels issued (graph replays count their nodes)
+    int* d_err = nullptr;              // set by a staged kernel whose bounded wait expired
 
-    void configure(int prec_, int dim_, int order_, const ShotDesc* d, int n, long long tiles, int maxrec,
-                   cudaStream_t s, int ctas_per_sm, int steps_per_graph) {
+    void configure(int prec_, int dim_, int order_, const ShotDesc* d, int n, long long tiles, long long tiles_s,
+                   int maxrec, cudaStream_t s, int ctas_per_sm, int steps_per_graph) {
         prec = prec_; dim = dim_; order = order_;
-        d_shots = d; nshots = n; ntiles = tiles; max_rec = maxrec; st = s;
+        d_shots = d; nshots = n; ntiles = tiles; ntiles_s = tiles_s; max_rec = maxrec; st = s;
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -31,6 +36,12 @@ struct Runner {
         long long gv = (long long)ov * sms, gt = (long long)ot * sms;
         grid_v = (int)(gv < tiles ? gv : (tiles > 0 ? tiles : 1));
         grid_t = (int)(gt < tiles ? gt : (tiles > 0 ? tiles : 1));
+        staged = staged_supported(prec, dim) && tiles_s > 0;
+        grid_s = (int)(sms < tiles_s ? sms : (tiles_s > 0 ? tiles_s : 1));
+        if (!d_err) {
+            if (cudaMalloc(&d_err, sizeof(int)) == cudaSuccess) cudaMemsetAsync(d_err, 0, sizeof(int), st);
+            else d_err = nullptr;
+        }
         graph_steps = steps_per_graph;
         reset_graph();
     }
@@ -41,14 +52,22 @@ struct Runner {
         graph = nullptr;
         graph_failed = false;
     }
-    ~Runner() { reset_graph(); }
+    ~Runner() {
+        reset_graph();
+        if (d_err) cudaFree(d_err);
+    }
+
+    cudaError_t phase(bool v, int k) {
+        if (staged) return launch_phase_staged(prec, order, v, d_shots, nshots, ntiles_s, k, grid_s, d_err, st);
+        return launch_phase(prec, dim, order, v, d_shots, nshots, ntiles, k, v ? grid_v : grid_t, st);
+    }
 
     // m steps issued directly (k = 0..m-1), then the step bases advance by m.
     cudaError_t issue(int m, bool count = true) {
         cudaError_t e = cudaSuccess;
         for (int k = 0; k < m && e == cudaSuccess; k++) {
-            e = launch_phase(prec, dim, order, true, d_shots, nshots, ntiles, k, grid_v, st);
-            if (e == cudaSuccess) e = launch_phase(prec, dim, order, false, d_shots, nshots, ntiles, k, grid_t, st);
+            e = phase(true, k);
+            if (e == cudaSuccess) e = phase(false, k);
             if (e == cudaSuccess) e = launch_post(prec, d_shots, nshots, max_rec, k, 1, st);
         }
         if (e == cudaSuccess) e = launch_advance(d_shots, nshots, m, st);
@@ -79,6 +98,13 @@ struct Runner {
         }
         if (m > 0 && e == cudaSuccess) e = issue(m);
         return e;
+    }
+    // BP_OK, or the error a staged kernel recorded (stream must be synchronised).
+    int device_error() const {
+        if (!d_err) return BP_OK;
+        int h = 0;
+        if (cudaMemcpy(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return BP_ERR_CUDA;
+        return h;
     }
 };
 

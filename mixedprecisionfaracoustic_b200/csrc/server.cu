@@ -228,6 +228,11 @@ static void server_loop(bp_server* s) {
 
 extern "C" {
 
+int bp_shot_bytes(const bp_config* cfg, size_t* bytes) {
+    if (!bytes) { set_error("bad arguments"); return BP_ERR_ARG; }
+    return Shot::plan_bytes(cfg, bytes);
+}
+
 int bp_server_create(int device, size_t hbm_budget, int steps_per_sync, bp_server** out) {
     if (!out || hbm_budget == 0 || steps_per_sync < 0) { set_error("bad arguments"); return BP_ERR_ARG; }
     *out = nullptr;

@@ -266,6 +266,8 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     S.nrows = p.ny * p.nz;
     S.tile0 = 0;
     S.rows_per_tile = tile_rows();
+    S.tile0s = 0;
+    S.nseg_s = (p.nx + staged_tile_width() - 1) / staged_tile_width();
     S.nt = c->nt;
     S.dt = c->dt; S.dtd = c->dt; S.h = c->dx; S.hd = c->dx; S.inv_h = 1.0f / c->dx;
     for (int f = 0; f < BP_NFIELDS; f++) { S.f[f] = at(p.o_f[f]); S.flo[f] = (int8_t*)at(p.o_flo[f]); }
@@ -402,6 +404,7 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     long long cx = p.nx - 2 * S.hw, cz = p.nz - 2 * S.hw, cy = dim == 3 ? p.ny - 2 * S.hw : 1;
     cells = cx * cy * cz;
     ntiles = (long long)S.nseg * ((S.nrows + tile_rows() - 1) / tile_rows());
+    ntiles_s = (long long)S.nseg_s * ((S.nrows + staged_tile_rows() - 1) / staged_tile_rows());
     it_host = 0;
     return BP_OK;
 }

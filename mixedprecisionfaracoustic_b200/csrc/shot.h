@@ -24,6 +24,12 @@ cudaError_t launch_coef(int prec, const ShotDesc* d_shots, int which, float* out
 int phase_threads();
 int tile_rows();
 int seg_cells();
+// TMA-staged 2D phase kernels (step_staged.cu)
+bool staged_supported(int prec, int dim);
+int staged_tile_rows();
+int staged_tile_width();
+cudaError_t launch_phase_staged(int prec, int order, bool vphase, const ShotDesc* d, int nshots, long long ntiles,
+                                int k, int grid, int* err, cudaStream_t st);
 int phase_occupancy(int prec, int dim, int order, bool vphase);
 
 void host_pml_region(int n, int np, float H, int i, bool* left, bool* right);
@@ -61,7 +67,8 @@ struct Shot {
     double* d_out = nullptr;           // 4 doubles
     long long cells = 0;               // updated cells per step
     int it_host = 0;                   // steps issued so far
-    long long ntiles = 0;
+    long long ntiles = 0;              // tiles of the register kernels (128 x 8)
+    long long ntiles_s = 0;            // tiles of the TMA-staged 2D kernels (256 x staged_tile_rows)
 
     // Computes the arena size for cfg without allocating (admission control).
     static int plan_bytes(const bp_config* cfg, size_t* bytes);

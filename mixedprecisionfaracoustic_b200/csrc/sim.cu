@@ -97,8 +97,8 @@ int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out) {
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); delete s; return BP_ERR_CUDA; }
     rc = s->shot.create(cfg, medium, s->st);
     if (rc) { s->shot.destroy(); cudaStreamDestroy(s->st); delete s; return rc; }
-    s->run.configure(cfg->precision, cfg->dim, cfg->order, s->shot.d_desc, 1, s->shot.ntiles, s->shot.nurec, s->st,
-                     0, 32);
+    s->run.configure(cfg->precision, cfg->dim, cfg->order, s->shot.d_desc, 1, s->shot.ntiles, s->shot.ntiles_s,
+                     s->shot.nurec, s->st, 0, 32);
     *out = s;
     return BP_OK;
 }
@@ -153,6 +153,8 @@ int bp_run_timed(bp_sim* s, int nsteps, float* ms) {
 int bp_sync(bp_sim* s) {
     if (!s) { set_error("null sim"); return BP_ERR_ARG; }
     SIM_CK(cudaStreamSynchronize(s->st));
+    int rc = s->run.device_error();
+    if (rc) { set_error("a staged phase kernel gave up waiting for its tile copies"); return rc; }
     return BP_OK;
 }
 

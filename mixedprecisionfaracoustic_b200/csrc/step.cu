@@ -36,10 +36,16 @@ __device__ __forceinline__ int locate_shot(const ShotDesc* shots, int nshots, lo
 
 template <class P>
 __device__ __forceinline__ typename P::real deriv_div(typename P::real a, const ShotDesc& S) {
-    // FP32/FP64 divide by H exactly like the reference; COMP16 multiplies by 1/H.
+    // FP32: the reference divides by H.  q = a * (1/H) refined by one residual
+    // step, q += (a - q H) * (1/H), with the exact fused residual a - q H,
+    // matches the IEEE quotient a / H to within one ulp (equal in all but rare
+    // near-tie cases) in 3 instructions instead of a full divide.
+    // FP64 divides; COMP16 (own arithmetic) multiplies by 1/H.
     if constexpr (P::prec == BP_PREC_FP64) return a / (typename P::real)S.hd;
-    else if constexpr (P::prec == BP_PREC_FP32) return a / S.h;
-    else return a * S.inv_h;
+    else if constexpr (P::prec == BP_PREC_FP32) {
+        const float q = a * S.inv_h;
+        return __fmaf_rn(__fmaf_rn(-q, S.h, a), S.inv_h, q);
+    } else return a * S.inv_h;
 }
 
 // Staggered difference from a span v[j] = f(x0 - HW + j).
@@ -621,9 +627,22 @@ __global__ void __launch_bounds__(kThreads) k_phase(const ShotDesc* __restrict__
                                                      long long ntiles, int k) {
     using R = typename P::real;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // The descriptor of the tile's shot is staged in shared memory whenever the
+    // shot changes, so the ~100 pointers and extents the chunk code reads are
+    // shared-memory broadcasts instead of per-warp global loads.
+    __shared__ ShotDesc sdesc;
+    int cur = -1;
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int si = nshots == 1 ? 0 : locate_shot(shots, nshots, t);
-        const ShotDesc& S = shots[si];
+        if (si != cur) {                      // uniform across the CTA
+            __syncthreads();
+            const long long* src = reinterpret_cast<const long long*>(shots + si);
+            long long* dst = reinterpret_cast<long long*>(&sdesc);
+            for (int w = threadIdx.x; w < (int)(sizeof(ShotDesc) / 8); w += blockDim.x) dst[w] = src[w];
+            __syncthreads();
+            cur = si;
+        }
+        const ShotDesc& S = sdesc;
         const int it = *S.step_base + k;
         if (S.done || it >= S.nt) continue;
         const long long lt = t - S.tile0;

@@ -49,20 +49,18 @@ def test_batch_shots_with_different_lengths():
 
 
 def test_server_invariance_and_admission():
+    """Requests submitted together into a budget that holds about three of them:
+    some queue until others finish (admission), several are resident at once
+    (continuous batching, 2D and 3D classes overlapping), and every result is
+    bit-identical to the same shot run alone."""
+    from mixedprecisionfaracoustic_b200.biot import shot_bytes
     reqs = config4_requests(seed=4, n=8, precision="fp32", scale=0.05, steps=(60, 200), include_3d=True)
     singles = [alone(c, m)[0] for c, m in reqs]
-    # budget that fits only a few shots at once: forces queueing + continuous batching
-    from mixedprecisionfaracoustic_b200 import _abi
-    import ctypes as C
-    sizes = []
-    for c, _ in reqs:
-        b = C.c_size_t()
-        sizes.append(c)
-    srv = Server(hbm_budget_bytes=256 << 20, steps_per_sync=20)
-    ids = []
-    for c, m in reqs:
-        ids.append(srv.submit(c, m))
-        time.sleep(0.01)
+    sizes = [shot_bytes(c) for c, _ in reqs]
+    budget = 3 * max(sizes)
+    assert sum(sizes) > budget
+    srv = Server(hbm_budget_bytes=budget, steps_per_sync=20)
+    ids = [srv.submit(c, m) for c, m in reqs]
     for rid in ids:
         srv.wait(rid, 300)
     for rid, ref in zip(ids, singles):

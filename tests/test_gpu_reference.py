@@ -56,6 +56,24 @@ def test_reference_text_format(ref_run, golden):
     assert sis.shape == (192, 501)
 
 
+def test_fp32_seismograms_match_reference_run():
+    """Full 3500-step drop-in run vs the reference's own sis*.dat (regenerated by
+    running the unmodified reference Float program on a B200; tests/golden/
+    float_ref_seismograms.npz keeps 26 of the 192 receiver rows)."""
+    from conftest import GOLDEN
+    g = np.load(GOLDEN / "float_ref_seismograms.npz")
+    rows = g["rows"]
+    cfg, med = reference_compat(nt=3500)
+    with Simulation(cfg, med) as s:
+        s.run(3500)
+        got = {k: s.traces(c)[rows] for k, c in (("sisx", "txx"), ("sisz", "tzz"), ("sisvu", "vux"),
+                                                 ("sisvw", "vwx"), ("sisp", "p"))}
+    for k in ("sisx", "sisz", "sisvu", "sisp"):
+        err = rel_l2(got[k], g[k])
+        assert err <= 1e-5, f"{k}: rel L2 {err:.3e}"
+    assert np.all(got["sisvw"] == 0) and np.all(g["sisvw"] == 0)   # receivers in the fluid borehole
+
+
 def test_comp16_reference_run_vs_fp64():
     cfg, med = reference_compat(nt=301, precision="comp16")
     c64, _ = reference_compat(nt=301, precision="fp64")
