@@ -52,6 +52,11 @@ def parse():
     ap.add_argument("--nz", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=20)
+    ap.add_argument("--workload", choices=["c1", "c3", "c4"], default="c1",
+                    help="c1: one 2D shot (default, the headline); c3: 64 batched 2D shots; c4: serving stream")
+    ap.add_argument("--scale", type=float, default=1.0, help="c3/c4: linear size scale of every shot")
+    ap.add_argument("--requests", type=int, default=200, help="c4: number of requests")
+    ap.add_argument("--precision", choices=["fp32", "comp16"], default="fp32", help="c3/c4 precision")
     ap.add_argument("--only", choices=["fp32", "comp16"], default=None,
                     help="time one precision only and skip the FP64, e2e and CPU legs (profiling runs)")
     return ap.parse_args()
@@ -292,9 +297,116 @@ def run_reference(args, rank, ws):
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_batch(args, rank, ws):
+    """c3: 64 2D shots (sizes from {1024^2, 1536x1024, 2048^2, 3072x1536}) in one
+    persistent launch per phase and graph-replayed chunks; this rank's share of
+    the shots (replicas.shard) when N > 1."""
+    import torch
+    from mixedprecisionfaracoustic_b200 import Batch
+    from mixedprecisionfaracoustic_b200.presets import config3_shots
+    from mixedprecisionfaracoustic_b200.replicas import max_over_ranks, my_shots, shot_cost
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    K, W = args.steps, args.warmup
+    shots = config3_shots(seed=3, nshots=64, nt=W + K + 400, precision=args.precision, scale=args.scale)
+    mine = my_shots([shot_cost(c) for c, _ in shots], rank, ws)
+    cfgs = [shots[i][0] for i in mine]
+    for c in cfgs:
+        c.device = dev
+    b = Batch(cfgs, [shots[i][1] for i in mine])
+    b.run(W)                   # includes the autotuner's timed candidate steps
+    b.sync()
+    u0 = b.cell_updates()
+    if ws > 1:
+        torch.distributed.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with ClockSampler(dev) as clk:
+        b.run(K)
+        b.sync()
+    el = max_over_ranks(time.perf_counter() - t0)
+    upd = b.cell_updates() - u0
+    tot = upd
+    if ws > 1:
+        t = torch.tensor([float(upd)], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t)
+        tot = int(t.item())
+    tune = b.tune()
+    b.close()
+    return {"metric": METRIC, "value": tot / el / 1e6, "unit": METRIC, "n_gpus": ws, "steps": K, "warmup": W,
+            "ms_per_step": el / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f16+i8 storage, f32 math", "data": "synthetic",
+            "config": {"workload": f"c3: 64 batched 2D shots x{args.scale} size, {args.precision}",
+                       "shots_on_rank0": len(mine), "tune": tune, "parallelism": f"shots sharded over {ws}"},
+            "clocks": clk.summary(), "timing": "host wall clock around bp_batch_run + bp_batch_sync"}
+
+
+def run_serve(args, rank):
+    """c4: Poisson stream of shot requests into the server at ~80% of its measured
+    capacity; p50/p99 latency and Mcell-updates/s (rank 0 only)."""
+    import torch
+    from mixedprecisionfaracoustic_b200 import Server
+    from mixedprecisionfaracoustic_b200.presets import config4_requests
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    reqs = config4_requests(seed=4, n=args.requests, precision=args.precision, scale=args.scale)
+    work = sum((c.padded[0] - 2) * max(c.padded[1] - 2, 1) * (c.padded[2] - 2) * c.nt for c, _ in reqs)
+    srv = Server(hbm_budget_bytes=150 << 30, steps_per_sync=100, device=dev)
+    # capacity probe: the first 8 requests back to back
+    t0 = time.perf_counter()
+    probe = [srv.submit(c, m) for c, m in reqs[:8]]
+    for r in probe:
+        srv.wait(r, 3600)
+    cap = sum((c.padded[0] - 2) * max(c.padded[1] - 2, 1) * (c.padded[2] - 2) * c.nt for c, _ in reqs[:8]) / (
+        time.perf_counter() - t0)
+    for r in probe:
+        srv.release(r)
+    rate = 0.8 * cap / (work / len(reqs))         # requests per second at 80% of capacity
+    rng = np.random.default_rng(4)
+    gaps = rng.exponential(1.0 / rate, len(reqs))
+    ids = []
+    t0 = time.perf_counter()
+    nxt = t0
+    for (c, m), g in zip(reqs, gaps):
+        nxt += g
+        while time.perf_counter() < nxt:
+            time.sleep(min(0.001, max(0.0, nxt - time.perf_counter())))
+        ids.append(srv.submit(c, m))
+    for r in ids:
+        srv.wait(r, 3600)
+    el = time.perf_counter() - t0
+    lat = sorted(srv.latency(r) for r in ids)
+    st = srv.stats()
+    srv.close()
+    return {"metric": METRIC, "value": work / el / 1e6, "unit": METRIC, "n_gpus": 1, "steps": None, "warmup": 8,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f16+i8 storage, f32 math", "data": "synthetic",
+            "config": {"workload": f"c4: {len(reqs)} Poisson requests x{args.scale} size, {args.precision}",
+                       "rate_per_s": rate, "capacity_cell_updates_per_s": cap, "hbm_budget_GB": 150},
+            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+            "server": {k: st[k] for k in ("completed", "max_resident", "busy_seconds", "cell_updates")},
+            "timing": "host wall clock from first submit to last completion"}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
+    if args.workload != "c1" and args.impl == "ours":
+        if ws > 1:
+            import torch
+            import torch.distributed as dist
+            from datetime import timedelta
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        out = run_batch(args, rank, ws) if args.workload == "c3" else (run_serve(args, rank) if rank == 0 else None)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
     if ws > 1:
         import torch
         import torch.distributed as dist

@@ -146,6 +146,18 @@ int bp_sync(bp_sim* sim);
  * and returns the device time of the nsteps steps in *ms. */
 int bp_run_timed(bp_sim* sim, int nsteps, float* ms);
 
+/* Steps captured per CUDA graph replay (default 32); 0 issues every step as
+ * direct launches. */
+int bp_set_graph_steps(bp_sim* sim, int steps);
+
+/* Phase-kernel family: BP_KERNEL_AUTO (the library's choice), BP_KERNEL_REGISTER
+ * (register-staged tiles, every dim/precision) or BP_KERNEL_STAGED (TMA
+ * bulk-copy staged tiles: 2D FP32/COMP16 only, else BP_ERR_ARG). */
+#define BP_KERNEL_AUTO 0
+#define BP_KERNEL_REGISTER 1
+#define BP_KERNEL_STAGED 2
+int bp_set_kernel(bp_sim* sim, int variant);
+
 /* Step index of the next step to run (it). */
 int bp_get_step(bp_sim* sim, int* it);
 

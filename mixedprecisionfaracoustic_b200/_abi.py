@@ -21,6 +21,7 @@ FIELD = {n: i for i, n in enumerate(FIELDS)}
 TRACES = ["txx", "tzz", "vux", "vwx", "p"]          # sisx sisz sisvu sisvw sisp
 TRACE = {n: i for i, n in enumerate(TRACES)}
 SRC_TAU, SRC_P = 1, 2
+KERNELS = {"auto": 0, "register": 1, "staged": 2}
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 COEFS = ["rho_x", "rho_y", "rho_z", "rhof", "cc1_x", "cc1_y", "cc1_z", "cc2_x", "cc2_y", "cc2_z",
          "C", "M", "H", "H2u", "mu_xy", "mu_xz", "mu_yz"]
@@ -70,6 +71,8 @@ _SIGS = [
     ("bp_run", C.c_int, [C.c_void_p, C.c_int]),
     ("bp_sync", C.c_int, [C.c_void_p]),
     ("bp_run_timed", C.c_int, [C.c_void_p, C.c_int, FloatP]),
+    ("bp_set_graph_steps", C.c_int, [C.c_void_p, C.c_int]),
+    ("bp_set_kernel", C.c_int, [C.c_void_p, C.c_int]),
     ("bp_get_step", C.c_int, [C.c_void_p, IntP]),
     ("bp_get_traces", C.c_int, [C.c_void_p, C.c_int, FloatP, C.c_size_t]),
     ("bp_get_snapshot", C.c_int, [C.c_void_p, C.c_int, C.c_int, FloatP, C.c_size_t]),

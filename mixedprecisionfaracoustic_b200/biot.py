@@ -189,6 +189,14 @@ class Simulation:
         check(self.lib.bp_run_timed(self.h, int(nsteps), C.byref(ms)), "bp_run_timed")
         return ms.value
 
+    def set_kernel(self, variant: str) -> None:
+        """Phase-kernel family: 'auto', 'register' or 'staged' (TMA, 2D FP32/COMP16)."""
+        check(self.lib.bp_set_kernel(self.h, _abi.KERNELS[variant]), "bp_set_kernel")
+
+    def set_graph_steps(self, steps: int) -> None:
+        """Steps per captured CUDA graph (0: direct launches)."""
+        check(self.lib.bp_set_graph_steps(self.h, int(steps)), "bp_set_graph_steps")
+
     @property
     def step(self) -> int:
         v = C.c_int()

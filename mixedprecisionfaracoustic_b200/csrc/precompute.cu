@@ -95,9 +95,82 @@ __device__ __forceinline__ void put(void* p, int8_t* lo, long long i, double v) 
     }
 }
 
-// Coefficient arrays of one shot.  The averaging runs over the reference's
-// range 1..N-2 (Float/main.cu:473-477); other cells keep 0.  For COMP16,
-// em/scales come from the exponent scan (k_scan_kr + host rounding).
+// ---- FP32: the reference's own float arithmetic (Float/main.cu:480-509 and
+// the per-step CC1/CC2 of :106-113), reproduced bit for bit with explicit
+// round-to-nearest intrinsics (no contraction), so the FP32 path starts from
+// exactly the coefficients the Float build uses.
+__device__ __forceinline__ float padf(const MediumDev& m, int k, int x, int y, int z) {
+    return (float)padded(m, k, x, y, z);
+}
+__device__ __forceinline__ float ref_harm4(float a, float b, float c, float d) {
+    if (a == 0.0f || b == 0.0f || c == 0.0f || d == 0.0f) return 0.0f;
+    const float s = __fadd_rn(__fadd_rn(__fadd_rn(__fdiv_rn(1.0f, a), __fdiv_rn(1.0f, b)), __fdiv_rn(1.0f, c)),
+                              __fdiv_rn(1.0f, d));
+    return (float)__ddiv_rn(1.0, __dmul_rn(0.25, (double)s));
+}
+struct Ref32Face {
+    float rho_x, c1, c2;
+};
+__device__ __forceinline__ Ref32Face ref32_face(const MediumDev& m, int x, int y, int z, int ax) {
+    const int x1 = x + (ax == 0), y1 = y + (ax == 1), z1 = z + (ax == 2);
+    Ref32Face f;
+    f.rho_x = __fdiv_rn(2.0f, __fadd_rn(padf(m, MD_RHO, x, y, z), padf(m, MD_RHO, x1, y1, z1)));
+    f.c1 = (float)__dmul_rn(0.5, (double)__fadd_rn(padf(m, MD_C1, x, y, z), padf(m, MD_C1, x1, y1, z1)));
+    f.c2 = (float)__dmul_rn(0.5, (double)__fadd_rn(padf(m, MD_C2, x, y, z), padf(m, MD_C2, x1, y1, z1)));
+    return f;
+}
+// CC1 = 0.5*C1*DT + C2 - rhof*rhof*rho (double sum, float product);
+// CC2 = (C2 - rhof*rhof*rho) [float] - 0.5*C1*DT [double]; CC1 = 0 marks C1 == 0.
+__device__ __forceinline__ void ref32_cc(float c1, float c2, float rhof, float rho, float DT, float& cc1, float& cc2) {
+    const float rr = __fmul_rn(__fmul_rn(rhof, rhof), rho);
+    const double h = __dmul_rn(__dmul_rn(0.5, (double)c1), (double)DT);
+    cc1 = c1 == 0.0f ? 0.0f : (float)__dsub_rn(__dadd_rn(h, (double)c2), (double)rr);
+    cc2 = (float)__dsub_rn((double)__fsub_rn(c2, rr), h);
+}
+
+__global__ void k_coefs_ref32(ShotDesc S, MediumDev m, float DT) {
+    const long long n = (long long)S.nx * S.ny * S.nz;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(q % S.nx);
+        const long long rest = q / S.nx;
+        const int y = (int)(rest % S.ny), z = (int)(rest / S.ny);
+        const long long i = x + (long long)y * S.pitch + (long long)z * S.plane;
+        const bool inner = x >= 1 && x < S.nx - 1 && z >= 1 && z < S.nz - 1 && (S.dim == 2 || (y >= 1 && y < S.ny - 1));
+        const float rhof = padf(m, MD_RHOF, x, y, z);
+        float* const* vc = reinterpret_cast<float* const*>(S.vc);
+        float* const* tc = reinterpret_cast<float* const*>(S.tc);
+        vc[VC_RHOF][i] = rhof;
+        tc[TC_C][i] = padf(m, MD_C, x, y, z);
+        tc[TC_M][i] = padf(m, MD_M, x, y, z);
+        tc[TC_H][i] = padf(m, MD_H, x, y, z);
+        tc[TC_H2U][i] = padf(m, MD_H2MU, x, y, z);
+        if (!inner) continue;   // outer cells are never updated: coefficients stay 0
+        const int rho_slot[3] = {VC_RHO_X, VC_RHO_Y, VC_RHO_Z};
+        const int c1_slot[3] = {VC_CC1_X, VC_CC1_Y, VC_CC1_Z};
+        const int c2_slot[3] = {VC_CC2_X, VC_CC2_Y, VC_CC2_Z};
+        for (int a = 0; a < 3; a++) {
+            if (a == 1 && S.dim == 2) continue;
+            const Ref32Face f = ref32_face(m, x, y, z, a);
+            float cc1, cc2;
+            ref32_cc(f.c1, f.c2, rhof, f.rho_x, DT, cc1, cc2);
+            vc[rho_slot[a]][i] = f.rho_x;
+            vc[c1_slot[a]][i] = cc1;
+            vc[c2_slot[a]][i] = cc2;
+        }
+        const float mu = padf(m, MD_MU, x, y, z);
+        tc[TC_MUXZ][i] = ref_harm4(mu, padf(m, MD_MU, x + 1, y, z), padf(m, MD_MU, x, y, z + 1), padf(m, MD_MU, x + 1, y, z + 1));
+        if (S.dim == 3) {
+            tc[TC_MUYZ][i] = ref_harm4(mu, padf(m, MD_MU, x, y + 1, z), padf(m, MD_MU, x, y, z + 1), padf(m, MD_MU, x, y + 1, z + 1));
+            tc[TC_MUXY][i] = ref_harm4(mu, padf(m, MD_MU, x + 1, y, z), padf(m, MD_MU, x, y + 1, z), padf(m, MD_MU, x + 1, y + 1, z));
+        }
+    }
+}
+
+// Coefficient arrays of one shot (FP64 precompute, COMP16 and FP64 paths).
+// The averaging runs over the reference's range 1..N-2 (Float/main.cu:473-477);
+// other cells keep 0.  For COMP16, em/scales come from the exponent scan
+// (k_scan_kr + host rounding).
 template <class P>
 __global__ void k_coefs(ShotDesc S, MediumDev m, double dt, int em) {
     const long long n = (long long)S.nx * S.ny * S.nz;
@@ -293,6 +366,45 @@ __global__ void k_profile(PmlGeom g, double dt, double v0, double rc, R* b, R* e
     e2[i] = (R)exp(-d2 * dt);
 }
 
+// FP32 tables exactly as the reference's host code forms them
+// (Float/main.cu:599-651): float positions and differences, double pow/exp
+// intermediates rounded to float, e = exp(float(-d DT)).  The FP32 path stores
+// b = float(-DT d) / 2, the double factor FD_V/FD_T apply (Float/main.cu:130).
+// Explicit _rn intrinsics keep the compiler from fusing any of it.
+__device__ __forceinline__ float ref_expf(float a) { return (float)exp((double)a); }
+__global__ void k_profile_ref32(PmlGeom g, float DT, float v0, float RC, float* b, float* e, float* b2, float* e2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    bool left, right;
+    pml_region(g, i, left, right);
+    const float H = g.H;
+    const float DP = __fmul_rn((float)g.np, H);
+    const float oleft = DP;
+    const float oright = __fsub_rn(__fmul_rn((float)(g.n - 1), H), DP);
+    const float x = __fmul_rn((float)i, H);
+    const float d0 = (float)__ddiv_rn(__dmul_rn(__dmul_rn(3.0, (double)v0), log(__ddiv_rn(1.0, (double)RC))),
+                                      __dmul_rn(2.0, (double)DP));
+    float d = 0.0f, d2 = 0.0f;
+    if (left) {
+        const float t = __fdiv_rn(__fsub_rn(oleft, x), DP);
+        const double u = __ddiv_rn(__dsub_rn((double)__fsub_rn(oleft, x), __dmul_rn(0.5, (double)H)), (double)DP);
+        d = (float)__dmul_rn((double)d0, __dmul_rn((double)t, (double)t));
+        d2 = (float)__dmul_rn((double)d0, __dmul_rn(u, u));
+    }
+    if (right) {
+        const float t = __fdiv_rn(__fsub_rn(x, oright), DP);
+        const double u = __ddiv_rn(__dsub_rn(__dadd_rn((double)x, __dmul_rn(0.5, (double)H)), (double)oright), (double)DP);
+        d = (float)__dmul_rn((double)d0, __dmul_rn((double)t, (double)t));
+        d2 = (float)__dmul_rn((double)d0, __dmul_rn(u, u));
+    }
+    const float ed = (left || right) ? ref_expf(__fmul_rn(-d, DT)) : 1.0f;
+    const float ed2 = (left || right) ? ref_expf(__fmul_rn(-d2, DT)) : 1.0f;
+    b[i] = __fmul_rn(__fmul_rn(-DT, d), 0.5f);
+    e[i] = ed;
+    b2[i] = __fmul_rn(__fmul_rn(-DT, d2), 0.5f);
+    e2[i] = ed2;
+}
+
 // ---------------------------------------------------------------------------
 // Host launchers
 void host_pml_region(int n, int np, float H, int i, bool* left, bool* right) {
@@ -307,7 +419,10 @@ cudaError_t launch_profile(int prec, int n, int np, float H, double dt, double v
                            void* b2, void* e2, cudaStream_t st) {
     PmlGeom g{n, np, H};
     int grid = (n + 255) / 256;
-    if (prec == BP_PREC_FP64)
+    if (prec == BP_PREC_FP32)
+        k_profile_ref32<<<grid, 256, 0, st>>>(g, (float)dt, (float)v0, (float)rc, (float*)b, (float*)e, (float*)b2,
+                                              (float*)e2);
+    else if (prec == BP_PREC_FP64)
         k_profile<double><<<grid, 256, 0, st>>>(g, dt, v0, rc, (double*)b, (double*)e, (double*)b2, (double*)e2);
     else
         k_profile<float><<<grid, 256, 0, st>>>(g, dt, v0, rc, (float*)b, (float*)e, (float*)b2, (float*)e2);
@@ -320,7 +435,7 @@ cudaError_t launch_coefs(int prec, const ShotDesc& S, const float* const* med, i
     for (int k = 0; k < 9; k++) m.a[k] = med[k];
     m.nx = pnx; m.ny = pny; m.nz = pnz; m.np = np;
     const int grid = 148 * 8;
-    if (prec == BP_PREC_FP32) k_coefs<PolF32><<<grid, 256, 0, st>>>(S, m, dt, em);
+    if (prec == BP_PREC_FP32) k_coefs_ref32<<<grid, 256, 0, st>>>(S, m, (float)dt);
     else if (prec == BP_PREC_COMP16) k_coefs<PolC16><<<grid, 256, 0, st>>>(S, m, dt, em);
     else k_coefs<PolF64><<<grid, 256, 0, st>>>(S, m, dt, em);
     return cudaGetLastError();

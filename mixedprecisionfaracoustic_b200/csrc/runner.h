@@ -23,6 +23,7 @@ struct Runner {
     bool graph_failed = false;
     long long launches = 0;            // kernels issued (graph replays count their nodes)
     int* d_err = nullptr;              // set by a staged kernel whose bounded wait expired
+    int variant = BP_KERNEL_AUTO;      // BP_KERNEL_*: which phase-kernel family runs
 
     void configure(int prec_, int dim_, int order_, const ShotDesc* d, int n, long long tiles, long long tiles_s,
                    int maxrec, cudaStream_t s, int ctas_per_sm, int steps_per_graph) {
@@ -36,7 +37,7 @@ struct Runner {
         long long gv = (long long)ov * sms, gt = (long long)ot * sms;
         grid_v = (int)(gv < tiles ? gv : (tiles > 0 ? tiles : 1));
         grid_t = (int)(gt < tiles ? gt : (tiles > 0 ? tiles : 1));
-        staged = staged_supported(prec, dim) && tiles_s > 0;
+        select_kernels();
         grid_s = (int)(sms < tiles_s ? sms : (tiles_s > 0 ? tiles_s : 1));
         if (!d_err) {
             if (cudaMalloc(&d_err, sizeof(int)) == cudaSuccess) cudaMemsetAsync(d_err, 0, sizeof(int), st);
@@ -44,6 +45,10 @@ struct Runner {
         }
         graph_steps = steps_per_graph;
         reset_graph();
+    }
+    void select_kernels() {
+        const bool can = staged_supported(prec, dim) && ntiles_s > 0;
+        staged = can && (variant == BP_KERNEL_STAGED || (variant == BP_KERNEL_AUTO && staged_default()));
     }
     void reset_graph() {
         if (exec) cudaGraphExecDestroy(exec);

@@ -26,6 +26,7 @@ int tile_rows();
 int seg_cells();
 // TMA-staged 2D phase kernels (step_staged.cu)
 bool staged_supported(int prec, int dim);
+bool staged_default();           // whether BP_KERNEL_AUTO picks the staged kernels where supported
 int staged_tile_rows();
 int staged_tile_width();
 cudaError_t launch_phase_staged(int prec, int order, bool vphase, const ShotDesc* d, int nshots, long long ntiles,

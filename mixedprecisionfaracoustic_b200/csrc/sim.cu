@@ -158,6 +158,27 @@ int bp_sync(bp_sim* s) {
     return BP_OK;
 }
 
+int bp_set_graph_steps(bp_sim* s, int steps) {
+    if (!s || steps < 0) { set_error("bad arguments"); return BP_ERR_ARG; }
+    SIM_CK(cudaStreamSynchronize(s->st));
+    s->run.graph_steps = steps;
+    s->run.reset_graph();
+    return BP_OK;
+}
+
+int bp_set_kernel(bp_sim* s, int variant) {
+    if (!s || variant < BP_KERNEL_AUTO || variant > BP_KERNEL_STAGED) { set_error("bad arguments"); return BP_ERR_ARG; }
+    if (variant == BP_KERNEL_STAGED && !staged_supported(s->shot.cfg.precision, s->shot.cfg.dim)) {
+        set_error("the staged kernels cover 2D FP32 and COMP16 only");
+        return BP_ERR_ARG;
+    }
+    SIM_CK(cudaStreamSynchronize(s->st));
+    s->run.variant = variant;
+    s->run.select_kernels();
+    s->run.reset_graph();
+    return BP_OK;
+}
+
 int bp_get_step(bp_sim* s, int* it) {
     if (!s || !it) { set_error("bad arguments"); return BP_ERR_ARG; }
     *it = s->shot.it_host;
@@ -285,9 +306,9 @@ int bp_profile_phases(bp_sim* s, int nsteps, float ms[3]) {
     cudaError_t e = cudaSuccess;
     for (int i = 0; i < nsteps && e == cudaSuccess; i++) {
         cudaEventRecord(ev[0], s->st);
-        e = launch_phase(R.prec, R.dim, R.order, true, R.d_shots, R.nshots, R.ntiles, 0, R.grid_v, s->st);
+        e = R.phase(true, 0);
         cudaEventRecord(ev[1], s->st);
-        if (e == cudaSuccess) e = launch_phase(R.prec, R.dim, R.order, false, R.d_shots, R.nshots, R.ntiles, 0, R.grid_t, s->st);
+        if (e == cudaSuccess) e = R.phase(false, 0);
         cudaEventRecord(ev[2], s->st);
         if (e == cudaSuccess) e = launch_post(R.prec, R.d_shots, R.nshots, R.max_rec, 0, 1, s->st);
         if (e == cudaSuccess) e = launch_advance(R.d_shots, R.nshots, 1, s->st);

@@ -144,17 +144,28 @@ template <int ORD, class P, bool V>
 __device__ __forceinline__ SPtrs stage_offsets(int i, int TR) {
     unsigned b = 0;
     SPtrs p{0, 0};
+#pragma unroll
     for (int k = 0; k < Arrays<ORD, V>::N; k++) {
-        SArr a = Arrays<ORD, V>::get(k, TR);
+        const SArr a = Arrays<ORD, V>::get(k, TR);
         const unsigned rows = a.r1 - a.r0 + 1, cells = span_cells(a.halo);
         if (k == i) {
             p.off_hi = b;
             p.off_lo = b + rows * cells * Elem<P>::hi;
-            return p;
         }
         b += rows * cells * (Elem<P>::hi + Elem<P>::lo);
     }
     return p;
+}
+
+// Total staged rows of a tile (over all arrays).
+template <int ORD, bool V>
+__host__ __device__ constexpr int total_rows(int TR) {
+    int n = 0;
+    for (int i = 0; i < Arrays<ORD, V>::N; i++) {
+        const SArr a = Arrays<ORD, V>::get(i, TR);
+        n += a.r1 - a.r0 + 1;
+    }
+    return n;
 }
 
 __device__ __forceinline__ const void* arr_ptr(const ShotDesc& S, const SArr& a, const int8_t** lo) {
@@ -183,42 +194,67 @@ __device__ __forceinline__ bool decode_tile(const ShotDesc* shots, int nshots, l
     return !S.done && it < S.nt;
 }
 
-// Issues the bulk copies of one tile into `stage`; returns the byte count.
-// With issue = false only counts (the expect_tx must precede the copies).
-template <int ORD, class P, bool V>
-__device__ unsigned tile_copies(const ShotDesc& S, int x0, int z0, int TR, unsigned char* stage, uint64_t* bar,
-                                bool issue) {
+// The bulk copies of one tile, spread over the 32 lanes of the producer warp:
+// lane l takes staged rows q = l, l+32, ... of the flattened (array, row)
+// list.  With issue = false it only returns the lane's byte count (the
+// warp-summed count is armed on the mbarrier before any copy is issued).
+template <int ORD, class P, bool V, int TR>
+__device__ __forceinline__ unsigned tile_copies_lane(const ShotDesc& S, int x0, int z0, unsigned char* stage,
+                                                     uint64_t* bar, int lane, bool issue) {
+    constexpr int NR = total_rows<ORD, V>(TR);
     unsigned total = 0;
-    for (int i = 0; i < Arrays<ORD, V>::N; i++) {
+    for (int q = lane; q < NR; q += 32) {
+        int i = 0, base = 0;
+        bool found = false;
+#pragma unroll
+        for (int k = 0; k < Arrays<ORD, V>::N; k++) {      // which array holds flat row q
+            const SArr a = Arrays<ORD, V>::get(k, TR);
+            const int rows = a.r1 - a.r0 + 1;
+            if (!found) {
+                if (q < base + rows) { i = k; found = true; }
+                else base += rows;
+            }
+        }
         const SArr a = Arrays<ORD, V>::get(i, TR);
+        const int r = a.r0 + (q - base);
+        const int z = z0 + r;
+        if (z < 0 || z >= S.nz) continue;
+        const int cells = span_cells(a.halo);
+        const int xs = a.halo ? x0 - kHalo : x0;       // first cell of the span
+        const int c0 = xs < 0 ? -xs : 0;               // cells clipped on the left
+        const int c1 = xs + cells > S.pitch ? S.pitch - xs : cells;
+        if (c1 <= c0) continue;
         const int8_t* lo;
         const void* hi = arr_ptr(S, a, &lo);
         const SPtrs sp = stage_offsets<ORD, P, V>(i, TR);
-        const int cells = span_cells(a.halo);
-        const int xs = a.halo ? x0 - kHalo : x0;       // first cell of the span
-        int c0 = xs < 0 ? -xs : 0;                     // cells clipped on the left
-        int c1 = cells;                                // one past the last cell
-        if (xs + c1 > S.pitch) c1 = S.pitch - xs;
-        if (c1 <= c0) continue;
-        for (int r = a.r0; r <= a.r1; r++) {
-            const int z = z0 + r;
-            if (z < 0 || z >= S.nz) continue;
-            const long long g = (long long)z * S.pitch + xs + c0;   // first copied cell
-            const unsigned nb = (unsigned)(c1 - c0);
-            const unsigned rowoff = (unsigned)(r - a.r0) * cells;
-            total += nb * Elem<P>::hi;
+        const long long g = (long long)z * S.pitch + xs + c0;   // first copied cell
+        const unsigned nb = (unsigned)(c1 - c0);
+        const unsigned rowoff = (unsigned)(r - a.r0) * cells;
+        total += nb * Elem<P>::hi;
+        if (issue)
+            bulk_g2s(stage + sp.off_hi + (rowoff + c0) * Elem<P>::hi,
+                     static_cast<const unsigned char*>(hi) + g * Elem<P>::hi, nb * Elem<P>::hi, bar);
+        if (Elem<P>::lo && lo) {
+            total += nb * Elem<P>::lo;
             if (issue)
-                bulk_g2s(stage + sp.off_hi + (rowoff + c0) * Elem<P>::hi,
-                         static_cast<const unsigned char*>(hi) + g * Elem<P>::hi, nb * Elem<P>::hi, bar);
-            if (Elem<P>::lo && lo) {
-                total += nb * Elem<P>::lo;
-                if (issue)
-                    bulk_g2s(stage + sp.off_lo + (rowoff + c0) * Elem<P>::lo,
-                             reinterpret_cast<const unsigned char*>(lo) + g * Elem<P>::lo, nb * Elem<P>::lo, bar);
-            }
+                bulk_g2s(stage + sp.off_lo + (rowoff + c0) * Elem<P>::lo,
+                         reinterpret_cast<const unsigned char*>(lo) + g * Elem<P>::lo, nb * Elem<P>::lo, bar);
         }
     }
     return total;
+}
+
+// Warp 0 arms `bar` with the tile's byte count and issues its copies.
+template <int ORD, class P, bool V, int TR>
+__device__ __forceinline__ void produce_tile(const ShotDesc& G, int x0, int z0, unsigned char* stage, uint64_t* bar,
+                                             int lane) {
+    fence_proxy_async();   // earlier generic reads of this stage before the async-proxy writes
+    unsigned bytes = tile_copies_lane<ORD, P, V, TR>(G, x0, z0, stage, bar, lane, false);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+    if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
+    __syncwarp();
+    tile_copies_lane<ORD, P, V, TR>(G, x0, z0, stage, bar, lane, true);
 }
 
 // Reads of staged values.
@@ -303,62 +339,61 @@ __device__ __forceinline__ void st_field(const ShotDesc& S, int f, long long i, 
 }
 
 // ---- the kernel --------------------------------------------------------------
-template <int ORD, class P, bool V, int TR>
+template <int ORD, class P, bool V, int TR, int NST>
 __global__ void __launch_bounds__(kSThreads, 1) k_phase_staged(const ShotDesc* __restrict__ shots, int nshots,
                                                                 long long ntiles, int k, int* err) {
     using R = typename P::real;
     static_assert(P::prec != BP_PREC_FP64, "FP64 runs the register kernel");
+    static_assert(NST >= 2 && NST <= 4, "2..4 stages");
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr unsigned SB = stage_bytes<ORD, P, V>(TR);
-    // stage q lives at smem + q * SB
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * SB);
+    // stage q lives at smem + q * SB; its mbarrier at bars[q]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + NST * SB);
     __shared__ ShotDesc sdesc;
     __shared__ int s_abort;
 
     const int tid = threadIdx.x;
     if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        for (int q = 0; q < NST; q++) mbar_init(&bars[q], 1);
         fence_mbar_init();
         s_abort = 0;
     }
     __syncthreads();
 
-    unsigned use0 = 0, use1 = 0;        // completed uses of each stage's barrier
-    // prologue: first tile's copies
-    long long t = blockIdx.x;
-    int si = 0, x0 = 0, z0 = 0;
-    bool act = t < ntiles ? decode_tile(shots, nshots, t, k, TR, si, x0, z0) : false;
-    if (tid == 0 && act) {
-        const ShotDesc& G = shots[si];
-        mbar_arrive_expect_tx(&bars[0], tile_copies<ORD, P, V>(G, x0, z0, TR, smem, &bars[0], false));
-        tile_copies<ORD, P, V>(G, x0, z0, TR, smem, &bars[0], true);
+    unsigned par = 0;                    // bit q: parity of the next completion of stage q
+    unsigned armed = 0;                  // bit q: stage q has copies outstanding
+    // prologue: the first NST-1 tiles of this CTA
+    for (int q = 0; q < NST - 1; q++) {
+        const long long tq = blockIdx.x + (long long)q * gridDim.x;
+        int a = 0, b = 0, c = 0;
+        if (tq < ntiles && decode_tile(shots, nshots, tq, k, TR, a, b, c)) {
+            if (tid < 32) produce_tile<ORD, P, V, TR>(shots[a], b, c, smem + q * SB, &bars[q], tid);
+            armed |= 1u << q;
+        }
     }
     int cur_shot = -1;
-    int s = 0;
-    for (; t < ntiles; t += gridDim.x, s ^= 1) {
-        // stage the descriptor of this tile's shot
-        if (act && si != cur_shot) {
+    int s = 0;                           // stage of the current tile
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, s = (s + 1 == NST ? 0 : s + 1)) {
+        // prefetch tile t + (NST-1) grid strides into the stage consumed last
+        // iteration (protected by the barrier that ended it)
+        const long long tn = t + (long long)(NST - 1) * gridDim.x;
+        const int sn = s == 0 ? NST - 1 : s - 1;
+        int sin = 0, x0n = 0, z0n = 0;
+        if (tn < ntiles && decode_tile(shots, nshots, tn, k, TR, sin, x0n, z0n)) {
+            if (tid < 32) produce_tile<ORD, P, V, TR>(shots[sin], x0n, z0n, smem + sn * SB, &bars[sn], tid);
+            armed |= 1u << sn;
+        }
+        int si = 0, x0 = 0, z0 = 0;
+        const bool act = decode_tile(shots, nshots, t, k, TR, si, x0, z0);
+        if (act && si != cur_shot) {     // stage the descriptor of this tile's shot
             const long long* src = reinterpret_cast<const long long*>(shots + si);
             long long* dst = reinterpret_cast<long long*>(&sdesc);
             for (int w = tid; w < (int)(sizeof(ShotDesc) / 8); w += blockDim.x) dst[w] = src[w];
         }
-        // prefetch the next tile into the other stage (its previous contents
-        // were consumed before the barrier that ended the last iteration)
-        const long long tn = t + gridDim.x;
-        int sin = 0, x0n = 0, z0n = 0;
-        const bool actn = tn < ntiles ? decode_tile(shots, nshots, tn, k, TR, sin, x0n, z0n) : false;
-        if (tid == 0 && actn) {
-            fence_proxy_async();
-            const ShotDesc& G = shots[sin];
-            mbar_arrive_expect_tx(&bars[s ^ 1], tile_copies<ORD, P, V>(G, x0n, z0n, TR, (smem + (s ^ 1) * SB), &bars[s ^ 1], false));
-            tile_copies<ORD, P, V>(G, x0n, z0n, TR, (smem + (s ^ 1) * SB), &bars[s ^ 1], true);
-        }
         __syncthreads();                 // sdesc ready
         if (act) {
-            if (!mbar_wait_bounded(&bars[s], (s ? use1 : use0) & 1u)) s_abort = 1;
-            else if (s) use1++;
-            else use0++;
+            if (!mbar_wait_bounded(&bars[s], (par >> s) & 1u)) s_abort = 1;
+            else { par ^= 1u << s; armed &= ~(1u << s); }
         }
         __syncthreads();
         if (s_abort) break;
@@ -484,48 +519,49 @@ __global__ void __launch_bounds__(kSThreads, 1) k_phase_staged(const ShotDesc* _
                 }
             }
         }
-        si = sin; x0 = x0n; z0 = z0n; act = actn;
         __syncthreads();                 // stage s fully read before it is refilled
     }
     if (s_abort) {
         // record the failure and drain copies still in flight (bounded) before exiting
         if (tid == 0) {
             atomicExch(err, BP_ERR_TIMEOUT);
-            mbar_wait_bounded(&bars[0], use0 & 1u);
-            mbar_wait_bounded(&bars[1], use1 & 1u);
+            for (int q = 0; q < NST; q++)
+                if (armed >> q & 1u) mbar_wait_bounded(&bars[q], (par >> q) & 1u);
         }
         __syncthreads();
     }
 }
 
 // ---- host side ---------------------------------------------------------------
-template <int ORD, class P, bool V, int TR>
+template <int ORD, class P, bool V, int TR, int NST>
 static cudaError_t launch_one(const ShotDesc* d, int nshots, long long ntiles, int k, int grid, int* err,
                               cudaStream_t st) {
-    const unsigned smem = 2 * stage_bytes<ORD, P, V>(TR) + 2 * sizeof(uint64_t);
+    const unsigned smem = NST * stage_bytes<ORD, P, V>(TR) + NST * sizeof(uint64_t);
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_phase_staged<ORD, P, V, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_phase_staged<ORD, P, V, TR, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    k_phase_staged<ORD, P, V, TR><<<grid, kSThreads, smem, st>>>(d, nshots, ntiles, k, err);
+    k_phase_staged<ORD, P, V, TR, NST><<<grid, kSThreads, smem, st>>>(d, nshots, ntiles, k, err);
     return cudaGetLastError();
 }
 
 constexpr int kTR = 4;
+constexpr int kStages = 3;   // prefetch distance 2 tiles; 3 x 73 KB (FP32 order 4 V) fits in 227 KB
 
 int staged_tile_rows() { return kTR; }
 int staged_tile_width() { return kSW; }
 
 bool staged_supported(int prec, int dim) { return dim == 2 && (prec == BP_PREC_FP32 || prec == BP_PREC_COMP16); }
+bool staged_default() { return false; }
 
 cudaError_t launch_phase_staged(int prec, int order, bool vphase, const ShotDesc* d, int nshots, long long ntiles,
                                 int k, int grid, int* err, cudaStream_t st) {
-#define BPS(O, PP)                                                                                   \
-    if (order == O) return vphase ? launch_one<O, PP, true, kTR>(d, nshots, ntiles, k, grid, err, st) \
-                                  : launch_one<O, PP, false, kTR>(d, nshots, ntiles, k, grid, err, st);
+#define BPS(O, PP)                                                                                       \
+    if (order == O) return vphase ? launch_one<O, PP, true, kTR, kStages>(d, nshots, ntiles, k, grid, err, st) \
+                                  : launch_one<O, PP, false, kTR, kStages>(d, nshots, ntiles, k, grid, err, st);
     if (prec == BP_PREC_FP32) { BPS(2, PolF32) BPS(4, PolF32) }
     if (prec == BP_PREC_COMP16) { BPS(2, PolC16) BPS(4, PolC16) }
 #undef BPS

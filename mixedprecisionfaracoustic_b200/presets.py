@@ -146,6 +146,55 @@ def config1(precision: str = "fp32", seed: int = 1, nx: int = 4000, nz: int = 20
     return cfg, med
 
 
+def lognormal_field(shape: tuple, sigma: float, corr: float, rng) -> np.ndarray:
+    """exp(sigma g - sigma^2/2) with g a unit-variance Gaussian field of correlation
+    length `corr` cells: white noise on a grid coarsened by corr/2, smoothed with a
+    Gaussian of one coarse cell, trilinearly upsampled and renormalised."""
+    from scipy import ndimage
+    step = max(1, int(round(corr / 2)))
+    cshape = tuple(s // step + 3 for s in shape)
+    g = ndimage.gaussian_filter(rng.standard_normal(cshape).astype(np.float32), sigma=1.0, mode="wrap")
+    g = ndimage.zoom(g, step, order=1)[tuple(slice(0, s) for s in shape)]
+    g = (g - g.mean()) / max(float(g.std()), 1e-12)
+    return np.exp(sigma * g - 0.5 * sigma * sigma).astype(np.float32)
+
+
+def config2(precision: str = "comp16", seed: int = 2, n=(512, 512, 384), npml: int = 20, nt: int = 3000,
+            order: int = 2, nrec_side: int = 256, sigma: float = 0.1, corr: float = 10.0):
+    """c2: 3D log-normal perturbation of the c0 moduli and permeability (scaled by n for tests)."""
+    nx, ny, nz = n
+    rng = np.random.default_rng(seed)
+    shape = (nz, ny, nx)
+    fkb, fmu, fks, fkap = (lognormal_field(shape, sigma, corr, rng) for _ in range(4))
+    p = C0
+    # per-cell Biot coefficients (the same formulas as bp_biot_from_moduli, vectorised)
+    Ks = p["Ks"] * fks.astype(np.float64)
+    Kb = np.minimum(p["Kb"] * fkb.astype(np.float64), 0.95 * Ks)
+    mu = p["mu"] * fmu.astype(np.float64)
+    kappa = p["kappa"] * fkap.astype(np.float64)
+    phi, Kf, rhos, rhof, tort, eta, m = p["phi"], p["Kf"], p["rhos"], p["rhof"], p["tort"], p["eta"], p["m_shape"]
+    alpha = 1 - Kb / Ks
+    M = Kf * Ks / (phi * Ks + (alpha - phi) * Kf)
+    H = alpha * alpha * M + Kb + mu * 4.0 / 3.0
+    med = Medium({"rho": np.full(shape, (1 - phi) * rhos + phi * rhof, np.float32),
+                  "rhof": np.full(shape, rhof, np.float32), "M": M.astype(np.float32),
+                  "C": (alpha * M).astype(np.float32), "H": H.astype(np.float32),
+                  "H2mu": (H - 2 * mu).astype(np.float32), "mu": mu.astype(np.float32),
+                  "C1": (eta / kappa).astype(np.float32),
+                  "C2": np.full(shape, (1 + 2 / m) * tort * rhof / phi, np.float32)})
+    vmax = float(np.sqrt(np.max(H) / ((1 - phi) * rhos + phi * rhof))) * 1.05
+    cx, cy = npml + nx // 2, npml + ny // 2
+    side = min(nrec_side, nx, ny)
+    xs = [npml + (i * nx) // side for i in range(side)]
+    ys = [npml + (j * ny) // side for j in range(side)]
+    rx = [x for y in ys for x in xs]
+    ry = [y for y in ys for _ in xs]
+    cfg = ShotConfig(dim=3, nx=nx, ny=ny, nz=nz, npml=npml, order=order, precision=precision, nt=nt, dx=DX, dt=DT,
+                     f0=20.0, pml_v0=vmax, pml_r=1e-6, src=(cx, cy, npml + 1), src_mask=_abi.SRC_TAU | _abi.SRC_P,
+                     rec_x=rx, rec_y=ry, rec_z=[npml + 1] * len(rx), check_cfl=1)
+    return cfg, med
+
+
 def config3_shots(seed: int = 3, nshots: int = 64, nt: int = 4000, precision: str = "fp32", npml: int = 20,
                   sizes=((1024, 1024), (1536, 1024), (2048, 2048), (3072, 1536)), order: int = 2,
                   scale: float = 1.0):

@@ -167,6 +167,7 @@ struct Oracle {
     int src_idx = -1;
 
     bool active_slot(const Slot& s) const { return dim == 3 || s.axis != 1; }
+    bool mode_ref() const { return REF; }
     bool field_used(int fidx) const {
         if (dim == 3) return true;
         return !(fidx == BP_F_VUY || fidx == BP_F_VWY || fidx == BP_F_TYY ||
@@ -592,11 +593,20 @@ float orc_load_ch(uint16_t hi, int8_t lo) {
     float h = orc_h2f(hi);
     return h + (float)lo * orc_residual_unit(h);
 }
+// The reference's store_ch is device code: its (int) conversion is the GPU's
+// saturating one (NaN -> 0, beyond range -> INT_MIN / INT_MAX), which decides
+// the residual when hi overflows to +-inf; x86's cvttss2si would give INT_MIN.
+static int device_f2i_rz(float x) {
+    if (x != x) return 0;
+    if (x >= 2147483648.0f) return 2147483647;
+    if (x <= -2147483648.0f) return (int)0x80000000u;
+    return (int)x;
+}
 void orc_store_ch(float v, uint16_t* hi, int8_t* lo) {
     uint16_t h = orc_f2h(v);
     float hf = orc_h2f(h);
     float scaled = (v - hf) / orc_residual_unit(hf);
-    int q = (int)(scaled + (scaled >= 0.0f ? 0.5f : -0.5f));
+    int q = device_f2i_rz(scaled + (scaled >= 0.0f ? 0.5f : -0.5f));
     if (q > 127) q = 127;
     if (q < -127) q = -127;
     *hi = h;
@@ -760,6 +770,32 @@ int orc_get_coef(void* hv, const char* name, double* out, size_t n) {
                                     &o->C2x, &o->C2y, &o->C2z, &o->cC, &o->cM, &o->cH, &o->cH2u,
                                     &o->muxy, &o->muxz, &o->muyz};
         rc = BP_ERR_NOT_FOUND;
+        // CC1/CC2 as FD_V forms them each step (Float/main.cu:106-113); the
+        // library stores CC1 = 0 where C1 == 0, so report that sentinel too
+        const char* ccn[6] = {"cc1x", "cc1y", "cc1z", "cc2x", "cc2y", "cc2z"};
+        for (int q = 0; q < 6; q++) {
+            if (std::strcmp(name, ccn[q])) continue;
+            const int a = q % 3;
+            auto* R = a == 0 ? &o->rhox : (a == 1 ? &o->rhoy : &o->rhoz);
+            auto* C1 = a == 0 ? &o->C1x : (a == 1 ? &o->C1y : &o->C1z);
+            auto* C2 = a == 0 ? &o->C2x : (a == 1 ? &o->C2y : &o->C2z);
+            if (R->empty() || n < o->ncell) { rc = BP_ERR_ARG; break; }
+            for (size_t i = 0; i < o->ncell; i++) {
+                const double r = (double)(*R)[i], c1 = (double)(*C1)[i], c2 = (double)(*C2)[i], rf = (double)o->rhof[i];
+                if (o->mode_ref()) {
+                    const float fr = (float)r, f1 = (float)c1, f2 = (float)c2, ff = (float)rf, DT = o->DT;
+                    const float cc1 = 0.5 * f1 * DT + f2 - ff * ff * fr;
+                    const float cc2 = f2 - ff * ff * fr - 0.5 * f1 * DT;
+                    out[i] = q < 3 ? (f1 == 0.0f ? 0.0 : (double)cc1) : (double)cc2;
+                } else {
+                    const double cc1 = 0.5 * c1 * o->DTd + c2 - rf * rf * r;
+                    const double cc2 = c2 - rf * rf * r - 0.5 * c1 * o->DTd;
+                    out[i] = q < 3 ? (c1 == 0.0 ? 0.0 : cc1) : cc2;
+                }
+            }
+            rc = 0;
+        }
+        if (rc == 0) break;
         for (int k = 0; k < 17; k++)
             if (!std::strcmp(name, names[k])) {
                 if (arr[k]->empty()) { rc = BP_ERR_NOT_FOUND; break; }

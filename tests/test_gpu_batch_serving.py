@@ -57,7 +57,7 @@ def test_server_invariance_and_admission():
     reqs = config4_requests(seed=4, n=8, precision="fp32", scale=0.05, steps=(60, 200), include_3d=True)
     singles = [alone(c, m)[0] for c, m in reqs]
     sizes = [shot_bytes(c) for c, _ in reqs]
-    budget = 3 * max(sizes)
+    budget = max(max(sizes), sum(sizes) // 3)
     assert sum(sizes) > budget
     srv = Server(hbm_budget_bytes=budget, steps_per_sync=20)
     ids = [srv.submit(c, m) for c, m in reqs]

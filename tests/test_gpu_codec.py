@@ -38,10 +38,10 @@ def test_scaled_coefficients_known_answers():
     """method.md 15.1-15.3 for the formation: 2^-em DT rho^-1 = 3.0381276459e-3,
     Aw = 0.9879429575, Bp = 2.0228360646e-4, 2^em DT H = 4.1182637215e-3,
     2^em DT C = 2.4139881134e-4, 2^em DT M = 2.4139881134e-3 (em = -23)."""
-    cfg, med = reference_compat(nt=4, n=(32, 32, 8), npml=8, precision="comp16")
+    cfg, med = reference_compat(nt=4, n=(32, 32, 24), npml=8, precision="comp16")
     with Simulation(cfg, med) as s:
         assert s.scaling()["em"] == -23
-        c = {n: s.coef(n)[4, 5, 5] for n in ("rho_x", "cc1_x", "cc2_x", "H", "C", "M")}
+        c = {n: s.coef(n)[12, 9, 9] for n in ("rho_x", "cc1_x", "cc2_x", "H", "C", "M")}
     ref = {"rho_x": 3.0381276459e-3, "cc1_x": 0.9879429575, "cc2_x": 2.0228360646e-4, "H": 4.1182637215e-3,
            "C": 2.4139881134e-4, "M": 2.4139881134e-3}
     for k, v in ref.items():
