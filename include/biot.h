@@ -235,6 +235,13 @@ int bp_comp16_decode(const uint16_t* hi, const int8_t* lo, size_t n, float* out)
  * n elements, accumulated in FP64 with warp-shuffle reductions.  Allocates
  * its reduction scratch on the device for the duration of the call. */
 int bp_rel_l2_device(const float* d_x, const float* d_ref, size_t n, double* rel);
+/* The same quantity without any device allocation (no counterpart in the
+ * reference).  The reduction scratch is a fixed 16 KB array in the library's
+ * device image, so n is limited to 16,777,216 elements (larger n returns
+ * BP_ERR_ARG).  The first call on a device, with that device current, looks up
+ * the array's address; make it before any stream capture begins.  Calls share
+ * that array: concurrent calls on one device race and must be serialised. */
+int bp_rel_l2_device_noalloc(const float* d_x, const float* d_ref, size_t n, double* rel);
 /* Relative L2 seismogram error of component comp of `x` against `ref` (same
  * receivers and nt), computed on the device in FP64. */
 int bp_trace_rel_l2(bp_sim* x, bp_sim* ref, int comp, double* rel);

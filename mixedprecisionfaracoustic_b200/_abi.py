@@ -91,6 +91,7 @@ _SIGS = [
     ("bp_comp16_encode", C.c_int, [FloatP, C.c_size_t, C.POINTER(C.c_uint16), C.POINTER(C.c_int8)]),
     ("bp_comp16_decode", C.c_int, [C.POINTER(C.c_uint16), C.POINTER(C.c_int8), C.c_size_t, FloatP]),
     ("bp_rel_l2_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, DoubleP]),
+    ("bp_rel_l2_device_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, DoubleP]),
     ("bp_trace_rel_l2", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, DoubleP]),
     ("bp_destroy", None, [C.c_void_p]),
     ("bp_error_string", C.c_char_p, [C.c_int]),
