@@ -151,11 +151,14 @@ int bp_run_timed(bp_sim* sim, int nsteps, float* ms);
 int bp_set_graph_steps(bp_sim* sim, int steps);
 
 /* Phase-kernel family: BP_KERNEL_AUTO (the library's choice), BP_KERNEL_REGISTER
- * (register-staged tiles, every dim/precision) or BP_KERNEL_STAGED (TMA
- * bulk-copy staged tiles: 2D FP32/COMP16 only, else BP_ERR_ARG). */
+ * (register-staged tiles, every dim/precision), BP_KERNEL_STAGED (TMA
+ * bulk-copy staged tiles: 2D FP32/COMP16 only, else BP_ERR_ARG) or
+ * BP_KERNEL_MARCH (warps marching along z with register windows: 2D
+ * FP32/COMP16 only, else BP_ERR_ARG).  All give bit-identical results. */
 #define BP_KERNEL_AUTO 0
 #define BP_KERNEL_REGISTER 1
 #define BP_KERNEL_STAGED 2
+#define BP_KERNEL_MARCH 3
 int bp_set_kernel(bp_sim* sim, int variant);
 
 /* Step index of the next step to run (it). */

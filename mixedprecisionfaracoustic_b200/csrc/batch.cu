@@ -42,14 +42,16 @@ int BatchCore::rebuild() {
     std::vector<ShotDesc> h(n);
     long long t0 = 0;
     int maxrec = 0;
-    long long t0s = 0;
+    long long t0s = 0, t0m = 0;
     for (int i = 0; i < n; i++) {
         h[i] = shots[i]->desc;
         h[i].tile0 = t0;
         h[i].tile0s = t0s;
+        h[i].tile0m = t0m;
         h[i].done = 0;
         t0 += shots[i]->ntiles;
         t0s += shots[i]->ntiles_s;
+        t0m += shots[i]->ntiles_m;
         maxrec = std::max(maxrec, shots[i]->nurec);
     }
     if (n > 0) {
@@ -57,7 +59,7 @@ int BatchCore::rebuild() {
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // h is a local buffer
         if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
     }
-    run.configure(prec, dim, order, d_descs, n, t0, t0s, maxrec, st, ctas_per_sm,
+    run.configure(prec, dim, order, d_descs, n, t0, t0s, t0m, maxrec, st, ctas_per_sm,
                   steps_per_sync > 0 ? steps_per_sync : 32);
     return BP_OK;
 }

@@ -89,6 +89,10 @@ struct ShotDesc {
     int src_rec;                  // receiver index that owns the source cell, or -1
     long long tile0s;             // first tile of this shot in the TMA-staged 2D tiling
     int nseg_s;                   // 256-cell segments per row in that tiling
+    int ncol_m;                   // marching 2D kernels: 128-cell columns per row
+    long long tile0m;             // first task of this shot in the marching tiling
+    int zseg_m;                   // rows per marching task
+    int pad_m;
     template <class R>
     __device__ __forceinline__ R dtr() const { return sizeof(R) == 8 ? (R)dtd : (R)dt; }
 };
@@ -162,6 +166,21 @@ struct PolF32 {
     __device__ __forceinline__ static void st1(void* p, int8_t*, long long i, real v) {
         static_cast<float*>(p)[i] = v;
     }
+    // raw (undecoded) loads, for kernels that issue loads well before use
+    using raw4 = float4;
+    using raw1 = float;
+    __device__ __forceinline__ static raw4 ldr4(const void* p, const int8_t*, long long i) {
+        return *reinterpret_cast<const float4*>(static_cast<const float*>(p) + i);
+    }
+    __device__ __forceinline__ static raw1 ldr1(const void* p, const int8_t*, long long i) {
+        return static_cast<const float*>(p)[i];
+    }
+    __device__ __forceinline__ static raw4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+    __device__ __forceinline__ static raw1 zero1() { return 0.f; }
+    __device__ __forceinline__ static void dec4(const raw4& t, real (&v)[4]) {
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
+    __device__ __forceinline__ static real dec1(raw1 t) { return t; }
 };
 
 struct PolF64 {
@@ -183,6 +202,21 @@ struct PolF64 {
     __device__ __forceinline__ static void st1(void* p, int8_t*, long long i, real v) {
         static_cast<double*>(p)[i] = v;
     }
+    struct raw4 { double2 a, b; };
+    using raw1 = double;
+    __device__ __forceinline__ static raw4 ldr4(const void* p, const int8_t*, long long i) {
+        const double2* q = reinterpret_cast<const double2*>(static_cast<const double*>(p) + i);
+        return raw4{q[0], q[1]};
+    }
+    __device__ __forceinline__ static raw1 ldr1(const void* p, const int8_t*, long long i) {
+        return static_cast<const double*>(p)[i];
+    }
+    __device__ __forceinline__ static raw4 zero4() { return raw4{make_double2(0, 0), make_double2(0, 0)}; }
+    __device__ __forceinline__ static raw1 zero1() { return 0.0; }
+    __device__ __forceinline__ static void dec4(const raw4& t, real (&v)[4]) {
+        v[0] = t.a.x; v[1] = t.a.y; v[2] = t.b.x; v[3] = t.b.y;
+    }
+    __device__ __forceinline__ static real dec1(raw1 t) { return t; }
 };
 
 // COMP16: fp16 hi (8 bytes per 4 cells) + int8 lo (4 bytes per 4 cells).
@@ -227,6 +261,41 @@ struct PolC16 {
         static_cast<__half*>(p)[i] = h;
         lo[i] = l;
     }
+    // raw loads: the fp16 words and the residual bytes (zero residuals where
+    // the array has none, which decodes to the same value as hi alone)
+    struct raw4 { uint2 h; char4 l; };
+    struct raw1 { __half h; int8_t l; };
+    __device__ __forceinline__ static raw4 ldr4(const void* p, const int8_t* lo, long long i) {
+        raw4 t;
+        t.h = *reinterpret_cast<const uint2*>(static_cast<const __half*>(p) + i);
+        t.l = lo ? *reinterpret_cast<const char4*>(lo + i) : make_char4(0, 0, 0, 0);
+        return t;
+    }
+    __device__ __forceinline__ static raw1 ldr1(const void* p, const int8_t* lo, long long i) {
+        raw1 t;
+        t.h = static_cast<const __half*>(p)[i];
+        t.l = lo ? lo[i] : (int8_t)0;
+        return t;
+    }
+    __device__ __forceinline__ static raw4 zero4() {
+        raw4 t;
+        t.h = make_uint2(0u, 0u);
+        t.l = make_char4(0, 0, 0, 0);
+        return t;
+    }
+    __device__ __forceinline__ static raw1 zero1() {
+        raw1 t;
+        t.h = __ushort_as_half((unsigned short)0);
+        t.l = 0;
+        return t;
+    }
+    __device__ __forceinline__ static void dec4(const raw4& t, real (&v)[4]) {
+        __half2 h01 = *reinterpret_cast<const __half2*>(&t.h.x);
+        __half2 h23 = *reinterpret_cast<const __half2*>(&t.h.y);
+        v[0] = decode_ch(__low2half(h01), t.l.x); v[1] = decode_ch(__high2half(h01), t.l.y);
+        v[2] = decode_ch(__low2half(h23), t.l.z); v[3] = decode_ch(__high2half(h23), t.l.w);
+    }
+    __device__ __forceinline__ static real dec1(const raw1& t) { return decode_ch(t.h, t.l); }
 };
 
 }  // namespace bpk

@@ -12,10 +12,11 @@ struct Runner {
     int prec = 0, dim = 2, order = 2;
     const ShotDesc* d_shots = nullptr;
     int nshots = 0;
-    long long ntiles = 0, ntiles_s = 0;
+    long long ntiles = 0, ntiles_s = 0, ntiles_m = 0;
     int max_rec = 0;
     int grid_v = 1, grid_t = 1, grid_s = 1;
     bool staged = false;
+    bool march = false;
     cudaStream_t st = nullptr;
     int graph_steps = 0;               // S; 0 disables graphs
     cudaGraph_t graph = nullptr;
@@ -26,9 +27,9 @@ struct Runner {
     int variant = BP_KERNEL_AUTO;      // BP_KERNEL_*: which phase-kernel family runs
 
     void configure(int prec_, int dim_, int order_, const ShotDesc* d, int n, long long tiles, long long tiles_s,
-                   int maxrec, cudaStream_t s, int ctas_per_sm, int steps_per_graph) {
+                   long long tiles_m, int maxrec, cudaStream_t s, int ctas_per_sm, int steps_per_graph) {
         prec = prec_; dim = dim_; order = order_;
-        d_shots = d; nshots = n; ntiles = tiles; ntiles_s = tiles_s; max_rec = maxrec; st = s;
+        d_shots = d; nshots = n; ntiles = tiles; ntiles_s = tiles_s; ntiles_m = tiles_m; max_rec = maxrec; st = s;
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -47,8 +48,10 @@ struct Runner {
         reset_graph();
     }
     void select_kernels() {
+        const bool can_m = march_supported(prec, dim) && ntiles_m > 0;
+        march = can_m && (variant == BP_KERNEL_MARCH || (variant == BP_KERNEL_AUTO && march_default()));
         const bool can = staged_supported(prec, dim) && ntiles_s > 0;
-        staged = can && (variant == BP_KERNEL_STAGED || (variant == BP_KERNEL_AUTO && staged_default()));
+        staged = !march && can && (variant == BP_KERNEL_STAGED || (variant == BP_KERNEL_AUTO && staged_default()));
     }
     void reset_graph() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -63,6 +66,7 @@ struct Runner {
     }
 
     cudaError_t phase(bool v, int k) {
+        if (march) return launch_phase_march(prec, order, v, d_shots, nshots, ntiles_m, k, st);
         if (staged) return launch_phase_staged(prec, order, v, d_shots, nshots, ntiles_s, k, grid_s, d_err, st);
         return launch_phase(prec, dim, order, v, d_shots, nshots, ntiles, k, v ? grid_v : grid_t, st);
     }

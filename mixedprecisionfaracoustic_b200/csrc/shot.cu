@@ -268,6 +268,14 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     S.rows_per_tile = tile_rows();
     S.tile0s = 0;
     S.nseg_s = (p.nx + staged_tile_width() - 1) / staged_tile_width();
+    S.tile0m = 0;
+    S.ncol_m = (p.nx + march_cells() - 1) / march_cells();
+    {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        S.zseg_m = march_zseg(S.ncol_m, p.nz - 2 * S.hw, sms);
+    }
     S.nt = c->nt;
     S.dt = c->dt; S.dtd = c->dt; S.h = c->dx; S.hd = c->dx; S.inv_h = 1.0f / c->dx;
     for (int f = 0; f < BP_NFIELDS; f++) { S.f[f] = at(p.o_f[f]); S.flo[f] = (int8_t*)at(p.o_flo[f]); }
@@ -405,6 +413,7 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     cells = cx * cy * cz;
     ntiles = (long long)S.nseg * ((S.nrows + tile_rows() - 1) / tile_rows());
     ntiles_s = (long long)S.nseg_s * ((S.nrows + staged_tile_rows() - 1) / staged_tile_rows());
+    ntiles_m = dim == 2 ? (long long)S.ncol_m * ((p.nz - 2 * S.hw + S.zseg_m - 1) / S.zseg_m) : 0;
     it_host = 0;
     return BP_OK;
 }

@@ -32,6 +32,13 @@ int staged_tile_width();
 cudaError_t launch_phase_staged(int prec, int order, bool vphase, const ShotDesc* d, int nshots, long long ntiles,
                                 int k, int grid, int* err, cudaStream_t st);
 int phase_occupancy(int prec, int dim, int order, bool vphase);
+// register-window marching 2D phase kernels (step_march.cu)
+bool march_supported(int prec, int dim);
+bool march_default();            // whether BP_KERNEL_AUTO picks the marching kernels where supported
+int march_cells();
+int march_zseg(long long ncol, int nrows, int sms);
+cudaError_t launch_phase_march(int prec, int order, bool vphase, const ShotDesc* d, int nshots, long long ntasks,
+                               int k, cudaStream_t st);
 
 void host_pml_region(int n, int np, float H, int i, bool* left, bool* right);
 cudaError_t launch_profile(int prec, int n, int np, float H, double dt, double v0, double rc, void* b, void* e,
@@ -70,6 +77,7 @@ struct Shot {
     int it_host = 0;                   // steps issued so far
     long long ntiles = 0;              // tiles of the register kernels (128 x 8)
     long long ntiles_s = 0;            // tiles of the TMA-staged 2D kernels (256 x staged_tile_rows)
+    long long ntiles_m = 0;            // tasks of the marching 2D kernels (128 cells x zseg_m rows)
 
     // Computes the arena size for cfg without allocating (admission control).
     static int plan_bytes(const bp_config* cfg, size_t* bytes);

@@ -98,7 +98,7 @@ int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out) {
     rc = s->shot.create(cfg, medium, s->st);
     if (rc) { s->shot.destroy(); cudaStreamDestroy(s->st); delete s; return rc; }
     s->run.configure(cfg->precision, cfg->dim, cfg->order, s->shot.d_desc, 1, s->shot.ntiles, s->shot.ntiles_s,
-                     s->shot.nurec, s->st, 0, 32);
+                     s->shot.ntiles_m, s->shot.nurec, s->st, 0, 32);
     *out = s;
     return BP_OK;
 }
@@ -167,9 +167,13 @@ int bp_set_graph_steps(bp_sim* s, int steps) {
 }
 
 int bp_set_kernel(bp_sim* s, int variant) {
-    if (!s || variant < BP_KERNEL_AUTO || variant > BP_KERNEL_STAGED) { set_error("bad arguments"); return BP_ERR_ARG; }
+    if (!s || variant < BP_KERNEL_AUTO || variant > BP_KERNEL_MARCH) { set_error("bad arguments"); return BP_ERR_ARG; }
     if (variant == BP_KERNEL_STAGED && !staged_supported(s->shot.cfg.precision, s->shot.cfg.dim)) {
         set_error("the staged kernels cover 2D FP32 and COMP16 only");
+        return BP_ERR_ARG;
+    }
+    if (variant == BP_KERNEL_MARCH && !march_supported(s->shot.cfg.precision, s->shot.cfg.dim)) {
+        set_error("the marching kernels cover 2D FP32 and COMP16 only");
         return BP_ERR_ARG;
     }
     SIM_CK(cudaStreamSynchronize(s->st));

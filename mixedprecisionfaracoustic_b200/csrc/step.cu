@@ -15,7 +15,7 @@
 // Neighbour rows (y, z) are re-read through L1/L2; DRAM sees each array once
 // per phase.  The CPML memory variables exist on the slabs only; a chunk
 // touches them only when it lies in a slab of that axis.
-#include "common.cuh"
+#include "stencil.cuh"
 
 namespace bpk {
 
@@ -34,173 +34,31 @@ __device__ __forceinline__ int locate_shot(const ShotDesc* shots, int nshots, lo
     return lo;
 }
 
+// Resident CTAs per SM the 2D FP32/COMP16 phase kernels are register-limited
+// to (1 = no limit).  Measured on B200 for the 4040 x 2040 order-2 grid: FP32
+// is fastest at 3 (80 registers, no spills); COMP16, whose decode/encode
+// chains leave it latency-bound, at 4 (64 registers, a few spilled values).
+#ifndef BP_MINB_F32
+#define BP_MINB_F32 3
+#endif
+#ifndef BP_MINB_C16
+#define BP_MINB_C16 4
+#endif
+template <int DIM, class P, bool VPHASE>
+__host__ __device__ constexpr int phase_min_blocks() {
+    return DIM != 2 ? 1 : P::prec == BP_PREC_FP32 ? BP_MINB_F32 : P::prec == BP_PREC_COMP16 ? BP_MINB_C16 : 1;
+}
+// How a tile learns its step index: 1 = once per shot per launch, 0 = a read
+// of the step counter per tile (measured faster for FP32 at 80 registers).
+#ifndef BP_TILE_LOOP_F32
+#define BP_TILE_LOOP_F32 0
+#endif
+#ifndef BP_TILE_LOOP_C16
+#define BP_TILE_LOOP_C16 1
+#endif
 template <class P>
-__device__ __forceinline__ typename P::real deriv_div(typename P::real a, const ShotDesc& S) {
-    // FP32: the reference divides by H.  q = a * (1/H) refined by one residual
-    // step, q += (a - q H) * (1/H), with the exact fused residual a - q H,
-    // matches the IEEE quotient a / H to within one ulp (equal in all but rare
-    // near-tie cases) in 3 instructions instead of a full divide.
-    // FP64 divides; COMP16 (own arithmetic) multiplies by 1/H.
-    if constexpr (P::prec == BP_PREC_FP64) return a / (typename P::real)S.hd;
-    else if constexpr (P::prec == BP_PREC_FP32) {
-        const float q = a * S.inv_h;
-        return __fmaf_rn(__fmaf_rn(-q, S.h, a), S.inv_h, q);
-    } else return a * S.inv_h;
-}
-
-// Staggered difference from a span v[j] = f(x0 - HW + j).
-template <int ORD, class R>
-__device__ __forceinline__ R dfwd(const R* v, int j) {   // at x0+j+1/2
-    constexpr int HW = ORD / 2;
-    if constexpr (ORD == 2) return v[HW + j + 1] - v[HW + j];
-    else return (R)1.125 * (v[HW + j + 1] - v[HW + j]) + (R)(-1.0 / 24.0) * (v[HW + j + 2] - v[HW + j - 1]);
-}
-template <int ORD, class R>
-__device__ __forceinline__ R dbwd(const R* v, int j) {   // at x0+j-1/2
-    constexpr int HW = ORD / 2;
-    if constexpr (ORD == 2) return v[HW + j] - v[HW + j - 1];
-    else return (R)1.125 * (v[HW + j] - v[HW + j - 1]) + (R)(-1.0 / 24.0) * (v[HW + j + 1] - v[HW + j - 2]);
-}
-// Difference across rows: a[k] = f(row + k - HW) for one cell.
-template <int ORD, class R>
-__device__ __forceinline__ R rfwd(const R* a) {
-    constexpr int HW = ORD / 2;
-    if constexpr (ORD == 2) return a[HW + 1] - a[HW];
-    else return (R)1.125 * (a[HW + 1] - a[HW]) + (R)(-1.0 / 24.0) * (a[HW + 2] - a[HW - 1]);
-}
-template <int ORD, class R>
-__device__ __forceinline__ R rbwd(const R* a) {
-    constexpr int HW = ORD / 2;
-    if constexpr (ORD == 2) return a[HW] - a[HW - 1];
-    else return (R)1.125 * (a[HW] - a[HW - 1]) + (R)(-1.0 / 24.0) * (a[HW + 1] - a[HW - 2]);
-}
-
-// Load f(x0 - HW .. x0 + 3 + HW) of one row; x neighbours clamped into the row
-// (clamped values only feed cells that are never updated).
-template <int ORD, class P>
-__device__ __forceinline__ void load_span(const void* p, const int8_t* lo, long long rowbase, int x0, int nx,
-                                          typename P::real (&v)[4 + ORD]) {
-    constexpr int HW = ORD / 2;
-    typename P::real c[4];
-    P::ld4(p, lo, rowbase + x0, c);
-#pragma unroll
-    for (int j = 0; j < 4; j++) v[HW + j] = c[j];
-#pragma unroll
-    for (int k = 1; k <= HW; k++) {
-        int xl = x0 - k; xl = xl < 0 ? 0 : xl;
-        int xr = x0 + 3 + k; xr = xr > nx - 1 ? nx - 1 : xr;
-        v[HW - k] = P::ld1(p, lo, rowbase + xl);
-        v[HW + 3 + k] = P::ld1(p, lo, rowbase + xr);
-    }
-}
-
-// Load the 4 cells of rows row-HW .. row+HW (offsets along y or z).
-template <int ORD, class P>
-__device__ __forceinline__ void load_rows(const void* p, const int8_t* lo, long long c, long long stride,
-                                          typename P::real (&a)[ORD + 1][4]) {
-    constexpr int HW = ORD / 2;
-#pragma unroll
-    for (int k = 0; k <= ORD; k++) P::ld4(p, lo, c + (long long)(k - HW) * stride, a[k]);
-}
-
-template <class R>
-__device__ __forceinline__ void scale4(R (&v)[4], R r) {
-#pragma unroll
-    for (int j = 0; j < 4; j++) v[j] *= r;
-}
-
-// CPML memory update of one derivative slot for a 4-cell chunk
-// (Float/main.cu:130-158):  ψ = ψ e + b (e prev + ∂),  prev = ∂,  ∂ += ψ,
-// with b = -DT d / 2 precomputed.  The x axis has per-cell tables; the y and z
-// axes one value per chunk.  Old ψ/prev are multiplied by the state rescale r.
-template <class R>
-__device__ __forceinline__ void cpml_x(R (&d)[4], R* psi, R* prev, const R* b, const R* e, int x0, R r) {
-    R ps[4], pv[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) { ps[j] = psi[j] * r; pv[j] = prev[j] * r; }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        R ee = e[x0 + j], bb = b[x0 + j];
-        R np = ps[j] * ee + bb * (ee * pv[j] + d[j]);
-        ps[j] = np;
-        pv[j] = d[j];
-        d[j] = d[j] + np;
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) { psi[j] = ps[j]; prev[j] = pv[j]; }
-}
-template <class R>
-__device__ __forceinline__ void cpml_s(R (&d)[4], R* psi, R* prev, R bb, R ee, R r) {
-    R ps[4], pv[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) { ps[j] = psi[j] * r; pv[j] = prev[j] * r; }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        R np = ps[j] * ee + bb * (ee * pv[j] + d[j]);
-        ps[j] = np;
-        pv[j] = d[j];
-        d[j] = d[j] + np;
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) { psi[j] = ps[j]; prev[j] = pv[j]; }
-}
-
-// Vector access helpers for the memory variables (ψ in fp32 or fp64).
-template <class R>
-struct PsiIO {
-    __device__ __forceinline__ static void ld(const R* p, R (&v)[4]) {
-        if constexpr (sizeof(R) == 4) {
-            float4 t = *reinterpret_cast<const float4*>(p);
-            v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-        } else {
-            double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
-            v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-        }
-    }
-    __device__ __forceinline__ static void st(R* p, const R (&v)[4]) {
-        if constexpr (sizeof(R) == 4) {
-            *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-        } else {
-            reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
-            reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
-        }
-    }
-};
-
-// One derivative slot of one axis: memory variables k (ψ) and NS+k (prev) of
-// the (phase, axis) slab array; fwd selects the half-grid profile.
-template <int NS, class R>
-__device__ __forceinline__ void cpml_slot(R (&d)[4], void* base, long long cells, int k, long long sidx,
-                                          bool xaxis, int pos, int x0, const void* pb, const void* pe, R r) {
-    R* ps = static_cast<R*>(base) + (long long)k * cells + sidx;
-    R* pv = static_cast<R*>(base) + (long long)(NS + k) * cells + sidx;
-    R psv[4], pvv[4];
-    PsiIO<R>::ld(ps, psv);
-    PsiIO<R>::ld(pv, pvv);
-    const R* b = static_cast<const R*>(pb);
-    const R* e = static_cast<const R*>(pe);
-    if (xaxis) cpml_x<R>(d, psv, pvv, b, e, x0, r);
-    else cpml_s<R>(d, psv, pvv, b[pos], e[pos], r);
-    PsiIO<R>::st(ps, psv);
-    PsiIO<R>::st(pv, pvv);
-}
-
-// Slab memory-variable index of a chunk for one axis, or -1 outside the slab.
-__device__ __forceinline__ long long slab_index(const ShotDesc& S, int axis, int x0, int y, int z) {
-    const Slab& sl = S.slab[axis];
-    if (axis == 0) {
-        int sx = sl.index(x0);
-        if (sx < 0) return -1;
-        return ((long long)z * S.ny + y) * sl.width + sx;
-    } else if (axis == 1) {
-        int sy = sl.index(y);
-        if (sy < 0) return -1;
-        return ((long long)z * sl.width + sy) * S.pitch + x0;
-    } else {
-        int sz = sl.index(z);
-        if (sz < 0) return -1;
-        return ((long long)sz * S.ny + y) * S.pitch + x0;
-    }
+__host__ __device__ constexpr bool step_once_per_shot() {
+    return P::prec == BP_PREC_COMP16 ? BP_TILE_LOOP_C16 : P::prec == BP_PREC_FP32 ? BP_TILE_LOOP_F32 : 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -213,9 +71,11 @@ __device__ __forceinline__ void v_chunk(const ShotDesc& S, int x0, int y, int z,
     const long long c = x0 + (long long)y * sy + (long long)z * sz;
     const long long row = c - x0;
 
+    VState<R> V;
+    auto &x1 = V.x1, &x3 = V.x3, &s1 = V.s1, &z1 = V.z1, &z2 = V.z2, &s3 = V.s3;
+    auto &x2 = V.x2, &y1 = V.y1, &y2 = V.y2, &y3 = V.y3, &s2 = V.s2, &z3 = V.z3;
+
     // ---- derivatives of the old stresses (x1..s3, Float/main.cu:115-128) ----
-    R x1[4], x3[4], s1[4], z1[4], z2[4], s3[4];
-    R x2[4], y1[4], y2[4], y3[4], s2[4], z3[4];
     {
         R v[4 + ORD];
         load_span<ORD, P>(S.f[BP_F_TXX], S.flo[BP_F_TXX], row, x0, S.nx, v);       // txx: D+x
@@ -282,102 +142,7 @@ __device__ __forceinline__ void v_chunk(const ShotDesc& S, int x0, int y, int z,
                 s2[j] = deriv_div<P>(rfwd<ORD>(t), S); }
         }
     }
-    // the rescale factor applies to old stresses: scale their derivatives
-    if constexpr (P::prec == BP_PREC_COMP16) {
-        scale4(x1, r); scale4(s1, r); scale4(z2, r); scale4(x3, r); scale4(z1, r); scale4(s3, r);
-        if constexpr (DIM == 3) { scale4(x2, r); scale4(y1, r); scale4(y2, r); scale4(y3, r); scale4(s2, r); scale4(z3, r); }
-    }
-    // masked cells (never updated) feed zero derivatives into the memory variables
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-        if (!(mask >> j & 1u)) {
-            x1[j] = 0; s1[j] = 0; z2[j] = 0; x3[j] = 0; z1[j] = 0; s3[j] = 0;
-            if constexpr (DIM == 3) { x2[j] = 0; y1[j] = 0; y2[j] = 0; y3[j] = 0; s2[j] = 0; z3[j] = 0; }
-        }
-
-    // ---- CPML memory variables on the slabs (Float/main.cu:130-158) ----
-    {
-        constexpr int NS = DIM == 3 ? 4 : 3;
-        long long si = slab_index(S, 0, x0, y, z);
-        if (si >= 0) {
-            void* B = S.psiV[0];
-            const long long n = S.slab_cells[0];
-            cpml_slot<NS, R>(x1, B, n, 0, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            cpml_slot<NS, R>(s1, B, n, 1, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            cpml_slot<NS, R>(z2, B, n, 2, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            if constexpr (DIM == 3) cpml_slot<NS, R>(y2, B, n, 3, si, true, x0, x0, S.pb[0], S.pe[0], r);
-        }
-        if constexpr (DIM == 3) {
-            si = slab_index(S, 1, x0, y, z);
-            if (si >= 0) {
-                void* B = S.psiV[1];
-                const long long n = S.slab_cells[1];
-                cpml_slot<NS, R>(x2, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, R>(y1, B, n, 1, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, R>(s2, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, R>(z3, B, n, 3, si, false, y, x0, S.pb[1], S.pe[1], r);
-            }
-        }
-        si = slab_index(S, 2, x0, y, z);
-        if (si >= 0) {
-            void* B = S.psiV[2];
-            const long long n = S.slab_cells[2];
-            cpml_slot<NS, R>(x3, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, R>(z1, B, n, 1, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            cpml_slot<NS, R>(s3, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            if constexpr (DIM == 3) cpml_slot<NS, R>(y3, B, n, 3, si, false, z, x0, S.pb[2], S.pe[2], r);
-        }
-    }
-
-    // ---- stress divergence per axis ----
-    R sumx[4], sumz[4], sumy[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        if constexpr (DIM == 3) {
-            sumx[j] = x1[j] + x2[j] + x3[j];
-            sumy[j] = y1[j] + y2[j] + y3[j];
-            sumz[j] = z1[j] + z2[j] + z3[j];
-        } else {
-            sumx[j] = x1[j] + x3[j];
-            sumz[j] = z1[j] + z2[j];
-        }
-    }
-
-    // ---- velocity updates per axis (Float/main.cu:106-113,160-190) ----
-    R rf[4];
-    P::ld4(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, rf);
-    auto axis_update = [&](const R (&sum)[4], const R (&dp)[4], int fu, int fw, int crho, int ccc1, int ccc2) {
-        R rho[4], c1[4], c2[4], vu[4], vw[4];
-        P::ld4(S.vc[crho], S.vclo[crho], c, rho);
-        P::ld4(S.vc[ccc1], S.vclo[ccc1], c, c1);
-        P::ld4(S.vc[ccc2], S.vclo[ccc2], c, c2);
-        P::ld4(S.f[fu], S.flo[fu], c, vu);
-        P::ld4(S.f[fw], S.flo[fw], c, vw);
-        R nu[4], nw[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16) {
-                // Half/main.cu:256-262 with Bt = (rhof rho^-1) Bp formed here
-                R wo = vw[j] * r, uo = vu[j] * r;
-                R rr = rf[j] * rho[j];                    // rhof * rho^-1
-                R wn = c1[j] * wo - (rr * c2[j]) * sum[j] - c2[j] * dp[j];
-                nw[j] = wn;
-                nu[j] = uo + rho[j] * sum[j] - rr * (wn - wo);
-            } else {
-                R wo = vw[j];
-                R wn = (c1[j] == (R)0) ? (R)0
-                                       : (wo * c2[j] - S.dtr<R>() * (rf[j] * rho[j] * sum[j] + dp[j])) / c1[j];
-                nw[j] = wn;
-                nu[j] = vu[j] + S.dtr<R>() * rho[j] * sum[j] - rf[j] * rho[j] * (wn - wo);
-            }
-            if (!(mask >> j & 1u)) { nw[j] = vw[j]; nu[j] = vu[j]; }
-        }
-        P::st4(S.f[fw], S.flo[fw], c, nw);
-        P::st4(S.f[fu], S.flo[fu], c, nu);
-    };
-    axis_update(sumx, s1, BP_F_VUX, BP_F_VWX, VC_RHO_X, VC_CC1_X, VC_CC2_X);
-    if constexpr (DIM == 3) axis_update(sumy, s2, BP_F_VUY, BP_F_VWY, VC_RHO_Y, VC_CC1_Y, VC_CC2_Y);
-    axis_update(sumz, s3, BP_F_VUZ, BP_F_VWZ, VC_RHO_Z, VC_CC1_Z, VC_CC2_Z);
+    v_tail<DIM, ORD, P, false>(S, c, x0, y, z, r, mask, V);
 }
 
 // ---------------------------------------------------------------------------
@@ -390,8 +155,10 @@ __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z,
     const long long c = x0 + (long long)y * sy + (long long)z * sz;
     const long long row = c - x0;
 
-    R uxx[4], uzz[4], wx[4], wz[4], uxz[4], uzx[4];
-    R uyy[4], wy[4], uxy[4], uyx[4], uyz[4], uzy[4];
+    TState<R> T;
+    auto &uxx = T.uxx, &uzz = T.uzz, &wx = T.wx, &wz = T.wz, &uxz = T.uxz, &uzx = T.uzx;
+    auto &uyy = T.uyy, &wy = T.wy, &uxy = T.uxy, &uyx = T.uyx, &uyz = T.uyz, &uzy = T.uzy;
+
     {
         R v[4 + ORD];
         R a[ORD + 1][4];
@@ -458,172 +225,13 @@ __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z,
                 uzy[j] = deriv_div<P>(rfwd<ORD>(t), S); }
         }
     }
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-        if (!(mask >> j & 1u)) {
-            uxx[j] = 0; wx[j] = 0; uzx[j] = 0; uzz[j] = 0; wz[j] = 0; uxz[j] = 0;
-            if constexpr (DIM == 3) { uyx[j] = 0; uyy[j] = 0; wy[j] = 0; uxy[j] = 0; uyz[j] = 0; uzy[j] = 0; }
-        }
-
-    // ---- CPML (Float/main.cu:252-285).  The velocities are this step's, but the
-    // stored ψ/prev of this phase are old state and take the rescale r ----
-    {
-        constexpr int NS = DIM == 3 ? 4 : 3;
-        long long si = slab_index(S, 0, x0, y, z);
-        if (si >= 0) {
-            void* B = S.psiT[0];
-            const long long n = S.slab_cells[0];
-            cpml_slot<NS, R>(uxx, B, n, 0, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            cpml_slot<NS, R>(wx, B, n, 1, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            cpml_slot<NS, R>(uzx, B, n, 2, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            if constexpr (DIM == 3) cpml_slot<NS, R>(uyx, B, n, 3, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-        }
-        if constexpr (DIM == 3) {
-            si = slab_index(S, 1, x0, y, z);
-            if (si >= 0) {
-                void* B = S.psiT[1];
-                const long long n = S.slab_cells[1];
-                cpml_slot<NS, R>(uyy, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, R>(wy, B, n, 1, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, R>(uxy, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, R>(uzy, B, n, 3, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-            }
-        }
-        si = slab_index(S, 2, x0, y, z);
-        if (si >= 0) {
-            void* B = S.psiT[2];
-            const long long n = S.slab_cells[2];
-            cpml_slot<NS, R>(uzz, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, R>(wz, B, n, 1, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, R>(uxz, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            if constexpr (DIM == 3) cpml_slot<NS, R>(uyz, B, n, 3, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-        }
-    }
-
-    // ---- pressure and stress updates (Float/main.cu:287-293) ----
-    R cC[4], cM[4], cH[4], cH2[4];
-    P::ld4(S.tc[TC_C], S.tclo[TC_C], c, cC);
-    P::ld4(S.tc[TC_M], S.tclo[TC_M], c, cM);
-    P::ld4(S.tc[TC_H], S.tclo[TC_H], c, cH);
-    P::ld4(S.tc[TC_H2U], S.tclo[TC_H2U], c, cH2);
-    const R dt = S.dtr<R>();
-    auto old4 = [&](int f, R (&v)[4]) {
-        P::ld4(S.f[f], S.flo[f], c, v);
-        if constexpr (P::prec == BP_PREC_COMP16) scale4(v, r);
-    };
-    auto store4 = [&](int f, R (&nv)[4], const R (&ov)[4]) {
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-            if (!(mask >> j & 1u)) nv[j] = ov[j];
-        P::st4(S.f[f], S.flo[f], c, nv);
-    };
-    R o[4], n[4];
-    if constexpr (DIM == 3) {
-        old4(BP_F_P, o);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16)
-                n[j] = o[j] - cC[j] * (uxx[j] + uyy[j] + uzz[j]) - cM[j] * (wx[j] + wy[j] + wz[j]);
-            else
-                n[j] = o[j] - dt * (cC[j] * (uxx[j] + uyy[j] + uzz[j]) + cM[j] * (wx[j] + wy[j] + wz[j]));
-        }
-        store4(BP_F_P, n, o);
-        old4(BP_F_TXX, o);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16)
-                n[j] = o[j] + cH2[j] * (uyy[j] + uzz[j]) + cH[j] * uxx[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
-            else
-                n[j] = o[j] + dt * (cH2[j] * (uyy[j] + uzz[j]) + cH[j] * uxx[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
-        }
-        store4(BP_F_TXX, n, o);
-        old4(BP_F_TYY, o);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16)
-                n[j] = o[j] + cH2[j] * (uxx[j] + uzz[j]) + cH[j] * uyy[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
-            else
-                n[j] = o[j] + dt * (cH2[j] * (uxx[j] + uzz[j]) + cH[j] * uyy[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
-        }
-        store4(BP_F_TYY, n, o);
-        old4(BP_F_TZZ, o);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16)
-                n[j] = o[j] + cH2[j] * (uxx[j] + uyy[j]) + cH[j] * uzz[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
-            else
-                n[j] = o[j] + dt * (cH2[j] * (uxx[j] + uyy[j]) + cH[j] * uzz[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
-        }
-        store4(BP_F_TZZ, n, o);
-        R mu[4];
-        P::ld4(S.tc[TC_MUXY], S.tclo[TC_MUXY], c, mu);
-        old4(BP_F_TXY, o);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16) n[j] = o[j] + mu[j] * (uxy[j] + uyx[j]);
-            else n[j] = o[j] + mu[j] * dt * (uxy[j] + uyx[j]);
-        }
-        store4(BP_F_TXY, n, o);
-        P::ld4(S.tc[TC_MUYZ], S.tclo[TC_MUYZ], c, mu);
-        old4(BP_F_TYZ, o);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16) n[j] = o[j] + mu[j] * (uyz[j] + uzy[j]);
-            else n[j] = o[j] + mu[j] * dt * (uyz[j] + uzy[j]);
-        }
-        store4(BP_F_TYZ, n, o);
-        P::ld4(S.tc[TC_MUXZ], S.tclo[TC_MUXZ], c, mu);
-        old4(BP_F_TXZ, o);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16) n[j] = o[j] + mu[j] * (uxz[j] + uzx[j]);
-            else n[j] = o[j] + mu[j] * dt * (uxz[j] + uzx[j]);
-        }
-        store4(BP_F_TXZ, n, o);
-    } else {
-        old4(BP_F_P, o);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16)
-                n[j] = o[j] - cC[j] * (uxx[j] + uzz[j]) - cM[j] * (wx[j] + wz[j]);
-            else
-                n[j] = o[j] - dt * (cC[j] * (uxx[j] + uzz[j]) + cM[j] * (wx[j] + wz[j]));
-        }
-        store4(BP_F_P, n, o);
-        old4(BP_F_TXX, o);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16)
-                n[j] = o[j] + cH2[j] * uzz[j] + cH[j] * uxx[j] + cC[j] * (wx[j] + wz[j]);
-            else
-                n[j] = o[j] + dt * (cH2[j] * uzz[j] + cH[j] * uxx[j] + cC[j] * (wx[j] + wz[j]));
-        }
-        store4(BP_F_TXX, n, o);
-        old4(BP_F_TZZ, o);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16)
-                n[j] = o[j] + cH2[j] * uxx[j] + cH[j] * uzz[j] + cC[j] * (wx[j] + wz[j]);
-            else
-                n[j] = o[j] + dt * (cH2[j] * uxx[j] + cH[j] * uzz[j] + cC[j] * (wx[j] + wz[j]));
-        }
-        store4(BP_F_TZZ, n, o);
-        R mu[4];
-        P::ld4(S.tc[TC_MUXZ], S.tclo[TC_MUXZ], c, mu);
-        old4(BP_F_TXZ, o);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if constexpr (P::prec == BP_PREC_COMP16) n[j] = o[j] + mu[j] * (uxz[j] + uzx[j]);
-            else n[j] = o[j] + mu[j] * dt * (uxz[j] + uzx[j]);
-        }
-        store4(BP_F_TXZ, n, o);
-    }
+    t_tail<DIM, ORD, P, false>(S, c, x0, y, z, r, mask, T);
 }
 
 // ---------------------------------------------------------------------------
 // Tile loop shared by both phases.
 template <int DIM, int ORD, class P, bool VPHASE>
-__global__ void __launch_bounds__(kThreads) k_phase(const ShotDesc* __restrict__ shots, int nshots,
+__global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, P, VPHASE>())) k_phase(const ShotDesc* __restrict__ shots, int nshots,
                                                      long long ntiles, int k) {
     using R = typename P::real;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -632,6 +240,8 @@ __global__ void __launch_bounds__(kThreads) k_phase(const ShotDesc* __restrict__
     // shared-memory broadcasts instead of per-warp global loads.
     __shared__ ShotDesc sdesc;
     int cur = -1;
+    bool live = false;
+    R r = (R)1;
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int si = nshots == 1 ? 0 : locate_shot(shots, nshots, t);
         if (si != cur) {                      // uniform across the CTA
@@ -641,13 +251,30 @@ __global__ void __launch_bounds__(kThreads) k_phase(const ShotDesc* __restrict__
             for (int w = threadIdx.x; w < (int)(sizeof(ShotDesc) / 8); w += blockDim.x) dst[w] = src[w];
             __syncthreads();
             cur = si;
+            if constexpr (step_once_per_shot<P>()) {
+                // the step index and the COMP16 rescale are fixed for the
+                // whole launch: read them once per shot, not once per tile
+                const int it = *sdesc.step_base + k;
+                live = !sdesc.done && it < sdesc.nt;
+                if constexpr (P::prec == BP_PREC_COMP16) r = live ? sdesc.rtab[it] : 1.0f;
+            }
         }
         const ShotDesc& S = sdesc;
-        const int it = *S.step_base + k;
-        if (S.done || it >= S.nt) continue;
-        const long long lt = t - S.tile0;
-        const int seg = (int)(lt % S.nseg);
-        const int row = (int)(lt / S.nseg) * kWarps + warp;
+        int seg, row;
+        if constexpr (step_once_per_shot<P>()) {
+            if (!live) continue;
+            const unsigned lt = (unsigned)(t - S.tile0);      // tiles of one shot < 2^32
+            const unsigned rb = lt / (unsigned)S.nseg;
+            seg = (int)(lt - rb * (unsigned)S.nseg);
+            row = (int)rb * kWarps + warp;
+        } else {
+            const int it = *S.step_base + k;
+            if (S.done || it >= S.nt) continue;
+            if constexpr (P::prec == BP_PREC_COMP16) r = S.rtab[it];
+            const long long lt = t - S.tile0;
+            seg = (int)(lt % S.nseg);
+            row = (int)(lt / S.nseg) * kWarps + warp;
+        }
         if (row >= S.nrows) continue;
         int y, z;
         if constexpr (DIM == 3) { y = row % S.ny; z = row / S.ny; }
@@ -661,8 +288,6 @@ __global__ void __launch_bounds__(kThreads) k_phase(const ShotDesc* __restrict__
 #pragma unroll
         for (int j = 0; j < 4; j++)
             if (x0 + j >= hw && x0 + j < S.nx - hw) mask |= 1u << j;
-        R r = (R)1;
-        if constexpr (P::prec == BP_PREC_COMP16) r = S.rtab[it];
         if constexpr (VPHASE) v_chunk<DIM, ORD, P>(S, x0, y, z, r, mask);
         else t_chunk<DIM, ORD, P>(S, x0, y, z, r, mask);
     }

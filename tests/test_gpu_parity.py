@@ -111,6 +111,31 @@ def test_staged_kernels_match_oracle_and_register_kernels(prec, order):
         assert rel_l2(out["staged"][c], out["register"][c]) <= (1e-6 if prec == "fp32" else 1e-4), c
 
 
+@pytest.mark.parametrize("prec,order", [("fp32", 2), ("fp32", 4), ("comp16", 2), ("comp16", 4)])
+@pytest.mark.parametrize("nx,nz", [(300, 70), (128, 41), (517, 150)])
+def test_march_kernels_bit_identical_to_register_kernels(prec, order, nx, nz):
+    """The z-marching 2D phase kernels compute the tile kernels' arithmetic on
+    the same operands: traces and every field bit-identical, on grids whose
+    width is, and is not, a multiple of the 128-cell column and whose height
+    splits into several z segments; and within tolerance of the oracle."""
+    cfg, med = small_2d(order, prec, nx=nx, nz=nz, nt=160)
+    out = {}
+    for variant in ("register", "march"):
+        with Simulation(cfg, med) as s:
+            s.set_kernel(variant)
+            s.run(cfg.nt)
+            out[variant] = ({c: s.traces(c) for c in _abi.TRACES},
+                            {f: s.field(f) for f in ("vux", "vuz", "vwx", "vwz", "p", "txx", "tzz", "txz")})
+    for c in _abi.TRACES:
+        assert np.array_equal(out["march"][0][c], out["register"][0][c]), c
+    for f in out["march"][1]:
+        assert np.array_equal(out["march"][1][f], out["register"][1][f]), f
+    ref = run_oracle(cfg, med, O.REF32 if prec == "fp32" else O.FP64)[0]
+    tol = 1e-5 if prec == "fp32" else 1e-3
+    for c in ("txx", "tzz", "vux", "p"):
+        assert rel_l2(out["march"][0][c], ref[c]) <= tol, (c, rel_l2(out["march"][0][c], ref[c]))
+
+
 def test_snapshots_match_oracle():
     cfg, med = small_3d(2, "fp32")
     with Simulation(cfg, med) as s:
