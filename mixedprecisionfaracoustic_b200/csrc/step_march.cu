@@ -24,15 +24,22 @@ constexpr int kMarchCells = 128;                 // x cells per task (4 per lane
 constexpr unsigned kFull = 0xffffffffu;
 // Resident CTAs per SM the marching kernels are register-limited to (1 = no
 // limit), and the warps per SM the z segments are sized for.  Measured on
-// B200 (4040 x 2040, order 2): 3 CTAs (168 registers) and 64 warps' worth of
-// segments (8-row segments) were the fastest settings tried; the kernel stays
-// slower than the tile kernels (occupancy-bound at 12 resident warps per SM,
-// with as many instructions per cell as theirs), so it is not the default.
+// B200 (4040 x 2040, order 2): the lean form below at 8 CTAs (64 registers)
+// with 8-row segments was the fastest setting tried (FP32 0.298, COMP16 0.474
+// ms per step); the kernel stays slower than the tile kernels (0.221 / 0.394),
+// so it is not the default.
 #ifndef BP_MARCH_MINB
-#define BP_MARCH_MINB 3
+#define BP_MARCH_MINB 8
 #endif
 #ifndef BP_MARCH_WARPS_PER_SM
 #define BP_MARCH_WARPS_PER_SM 64
+#endif
+// 1: no look-ahead; the coefficients and old state are loaded by the shared
+// tail after the derivatives (as in the tile kernels), which keeps only the
+// z windows live across rows.  0: row z+1's loads are all issued before row z
+// is computed.
+#ifndef BP_MARCH_LEAN
+#define BP_MARCH_LEAN 1
 #endif
 
 // Binary search of the shot owning task t (tile0m ascending).
@@ -169,7 +176,7 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
             typename P::raw4 txx, p, zz, xz, rf, rho_x, c1_x, c2_x, vu_x, vw_x, rho_z, c1_z, c2_z, vu_z, vw_z;
             Edges<ORD, P> etxx, ep, exz;
         };
-        auto issue = [&](int z, Row& L) {
+        auto issue_stress = [&](int z, Row& L) {
             const long long c = at(z), rb = (long long)z * sz;
             L.txx = ldr_row<P>(S.f[BP_F_TXX], S.flo[BP_F_TXX], c, in);
             L.p = ldr_row<P>(S.f[BP_F_P], S.flo[BP_F_P], at(z + HW), in);
@@ -178,6 +185,9 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
             ldr_edges<ORD, P>(S.f[BP_F_TXX], S.flo[BP_F_TXX], rb, x0, nx, lane, L.etxx);
             ldr_edges<ORD, P>(S.f[BP_F_P], S.flo[BP_F_P], rb, x0, nx, lane, L.ep);
             ldr_edges<ORD, P>(S.f[BP_F_TXZ], S.flo[BP_F_TXZ], rb, x0, nx, lane, L.exz);
+        };
+        auto issue_coef = [&](int z, Row& L) {
+            const long long c = at(z);
             L.rf = ldr_row<P>(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, in);
             L.rho_x = ldr_row<P>(S.vc[VC_RHO_X], S.vclo[VC_RHO_X], c, in);
             L.c1_x = ldr_row<P>(S.vc[VC_CC1_X], S.vclo[VC_CC1_X], c, in);
@@ -198,11 +208,13 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
             P::dec4(ldr_row<P>(S.f[BP_F_TZZ], S.flo[BP_F_TZZ], at(zb - HW + 1 + w), in), wzz[w]);
             P::dec4(ldr_row<P>(S.f[BP_F_TXZ], S.flo[BP_F_TXZ], at(zb - HW + w), in), wxz[w]);
         }
+        constexpr bool kLean = BP_MARCH_LEAN;
         Row L;
-        issue(zb, L);
+        if constexpr (!kLean) { issue_stress(zb, L); issue_coef(zb, L); }
         for (int z = zb; z < ze; z++) {
             Row N;
-            if (z + 1 < ze) issue(z + 1, N);          // next row in flight during this one
+            if constexpr (kLean) issue_stress(z, L);
+            else if (z + 1 < ze) { issue_stress(z + 1, N); issue_coef(z + 1, N); }   // next row in flight
             const long long c = at(z);
             R ct[4];
             P::dec4(L.txx, ct);
@@ -210,11 +222,13 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
             P::dec4(L.zz, wzz[ORD - 1]);
             P::dec4(L.xz, wxz[ORD - 1]);
             VState<R> V;
-            P::dec4(L.rf, V.rf);
-            P::dec4(L.rho_x, V.rho_x); P::dec4(L.c1_x, V.c1_x); P::dec4(L.c2_x, V.c2_x);
-            P::dec4(L.vu_x, V.vu_x); P::dec4(L.vw_x, V.vw_x);
-            P::dec4(L.rho_z, V.rho_z); P::dec4(L.c1_z, V.c1_z); P::dec4(L.c2_z, V.c2_z);
-            P::dec4(L.vu_z, V.vu_z); P::dec4(L.vw_z, V.vw_z);
+            if constexpr (!kLean) {
+                P::dec4(L.rf, V.rf);
+                P::dec4(L.rho_x, V.rho_x); P::dec4(L.c1_x, V.c1_x); P::dec4(L.c2_x, V.c2_x);
+                P::dec4(L.vu_x, V.vu_x); P::dec4(L.vw_x, V.vw_x);
+                P::dec4(L.rho_z, V.rho_z); P::dec4(L.c1_z, V.c1_z); P::dec4(L.c2_z, V.c2_z);
+                P::dec4(L.vu_z, V.vu_z); P::dec4(L.vw_z, V.vw_z);
+            }
             // derivatives of the old stresses (Float/main.cu:115-128)
             R v[4 + ORD];
             span_of<ORD, P>(ct, L.etxx, lane, v);                     // txx: D+x
@@ -232,11 +246,11 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
                 V.z1[j] = dz_fwd<ORD, P>(wzz, j, S);                   // tzz: D+z
                 V.s3[j] = dz_fwd<ORD, P>(wp, j, S);                    // p: D+z
             }
-            if (act) v_tail<2, ORD, P, true>(S, c, x0, 0, z, r, mask, V);
+            if (act) v_tail<2, ORD, P, !kLean>(S, c, x0, 0, z, r, mask, V);
             shift(wp);
             shift(wzz);
             shift(wxz);
-            L = N;
+            if constexpr (!kLean) L = N;
         }
     } else {
         // loaded one row ahead: vwx(z); the newest window rows vux(z+HW),
@@ -246,7 +260,7 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
             typename P::raw4 wx, ux, uz, wz, cC, cM, cH, cH2, mxz, op, oxx, ozz, oxz;
             Edges<ORD, P> eux, ewx, euz;
         };
-        auto issue = [&](int z, Row& L) {
+        auto issue_vel = [&](int z, Row& L) {
             const long long c = at(z), rb = (long long)z * sz;
             L.wx = ldr_row<P>(S.f[BP_F_VWX], S.flo[BP_F_VWX], c, in);
             L.ux = ldr_row<P>(S.f[BP_F_VUX], S.flo[BP_F_VUX], at(z + HW), in);
@@ -255,6 +269,9 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
             ldr_edges<ORD, P>(S.f[BP_F_VUX], S.flo[BP_F_VUX], rb, x0, nx, lane, L.eux);
             ldr_edges<ORD, P>(S.f[BP_F_VWX], S.flo[BP_F_VWX], rb, x0, nx, lane, L.ewx);
             ldr_edges<ORD, P>(S.f[BP_F_VUZ], S.flo[BP_F_VUZ], rb, x0, nx, lane, L.euz);
+        };
+        auto issue_coef = [&](int z, Row& L) {
+            const long long c = at(z);
             L.cC = ldr_row<P>(S.tc[TC_C], S.tclo[TC_C], c, in);
             L.cM = ldr_row<P>(S.tc[TC_M], S.tclo[TC_M], c, in);
             L.cH = ldr_row<P>(S.tc[TC_H], S.tclo[TC_H], c, in);
@@ -273,11 +290,13 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
             P::dec4(ldr_row<P>(S.f[BP_F_VUZ], S.flo[BP_F_VUZ], at(zb - HW + w), in), wuz[w]);
             P::dec4(ldr_row<P>(S.f[BP_F_VWZ], S.flo[BP_F_VWZ], at(zb - HW + w), in), wwz[w]);
         }
+        constexpr bool kLean = BP_MARCH_LEAN;
         Row L;
-        issue(zb, L);
+        if constexpr (!kLean) { issue_vel(zb, L); issue_coef(zb, L); }
         for (int z = zb; z < ze; z++) {
             Row N;
-            if (z + 1 < ze) issue(z + 1, N);
+            if constexpr (kLean) issue_vel(z, L);
+            else if (z + 1 < ze) { issue_vel(z + 1, N); issue_coef(z + 1, N); }
             const long long c = at(z);
             R cwx[4];
             P::dec4(L.wx, cwx);
@@ -285,11 +304,13 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
             P::dec4(L.uz, wuz[ORD - 1]);
             P::dec4(L.wz, wwz[ORD - 1]);
             TState<R> T;
-            P::dec4(L.cC, T.cC); P::dec4(L.cM, T.cM); P::dec4(L.cH, T.cH); P::dec4(L.cH2, T.cH2);
-            P::dec4(L.mxz, T.mxz);
-            P::dec4(L.op, T.op); P::dec4(L.oxx, T.oxx); P::dec4(L.ozz, T.ozz); P::dec4(L.oxz, T.oxz);
-            if constexpr (P::prec == BP_PREC_COMP16) {    // old state takes this step's rescale
-                scale4(T.op, r); scale4(T.oxx, r); scale4(T.ozz, r); scale4(T.oxz, r);
+            if constexpr (!kLean) {
+                P::dec4(L.cC, T.cC); P::dec4(L.cM, T.cM); P::dec4(L.cH, T.cH); P::dec4(L.cH2, T.cH2);
+                P::dec4(L.mxz, T.mxz);
+                P::dec4(L.op, T.op); P::dec4(L.oxx, T.oxx); P::dec4(L.ozz, T.ozz); P::dec4(L.oxz, T.oxz);
+                if constexpr (P::prec == BP_PREC_COMP16) {    // old state takes this step's rescale
+                    scale4(T.op, r); scale4(T.oxx, r); scale4(T.ozz, r); scale4(T.oxz, r);
+                }
             }
             // derivatives of this step's velocities (Float/main.cu:236-250)
             R v[4 + ORD];
@@ -308,11 +329,11 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
                 T.wz[j] = dz_bwd<ORD, P>(wwz, j, S);                    // vwz: D-z
                 T.uxz[j] = dz_fwd<ORD, P>(wux, j, S);                   // vux: D+z
             }
-            if (act) t_tail<2, ORD, P, true>(S, c, x0, 0, z, r, mask, T);
+            if (act) t_tail<2, ORD, P, !kLean>(S, c, x0, 0, z, r, mask, T);
             shift(wux);
             shift(wuz);
             shift(wwz);
-            L = N;
+            if constexpr (!kLean) L = N;
         }
     }
 }
