@@ -211,6 +211,37 @@ int bp_get_scaling(bp_sim* sim, int* em, int* es, float* dyn_scale,
  * (Float/main.cu:1187-1222). */
 int bp_write_reference_outputs(bp_sim* sim, const char* dir);
 
+/* The same outputs in binary (no counterpart in the reference, whose only
+ * format is the text above): traces.bin holds all five components
+ * [BP_NTRACE][nrec][nt]; one <field><it>.bin per captured snapshot field
+ * ([NZe][NXe] slice or [NZe][NYe][NXe] volume).  Each file is a 32-byte
+ * header {char magic[8] = "BPBIN001"; int32 version = 1, dtype = 0 (float32),
+ * ndims, dims[3]} followed by the little-endian float32 array, last dimension
+ * fastest. */
+int bp_write_binary_outputs(bp_sim* sim, const char* dir);
+
+/* Streaming of large receiver sets (no counterpart in the reference): the
+ * device keeps one trace per distinct receiver cell; bp_receiver_map gives
+ * their count and, if map is not null, the distinct-cell index of each of
+ * the nrec receivers.  bp_copy_traces_async enqueues on the simulation's
+ * stream, after the steps already issued, the copy of steps [it0, it0 + n)
+ * of component comp for every distinct cell into host[nurec][n]; it returns
+ * at once (pass page-locked memory for an asynchronous copy) and bp_sync
+ * waits for it. */
+int bp_receiver_map(bp_sim* sim, int* nurec, int* map);
+int bp_copy_traces_async(bp_sim* sim, int comp, int it0, int n, float* host);
+
+/* Checkpoint of the simulation's evolving state (no counterpart in the
+ * reference): wavefields, CPML memory variables, traces and snapshots
+ * recorded so far, and the step index.  bp_checkpoint_size gives the image
+ * size; bp_checkpoint waits for the issued steps and copies the image into
+ * host memory; bp_restore loads an image into a simulation created with the
+ * same configuration and medium (BP_ERR_ARG otherwise), after which bp_run
+ * continues exactly as the checkpointed simulation would have. */
+int bp_checkpoint_size(bp_sim* sim, size_t* bytes);
+int bp_checkpoint(bp_sim* sim, void* host, size_t bytes);
+int bp_restore(bp_sim* sim, const void* host, size_t bytes);
+
 /* Times nsteps steps phase by phase with CUDA events on the simulation's
  * stream and returns the mean device time (ms) of each phase:
  * ms[0] = V phase (velocity + its CPML), ms[1] = T phase (stress, pressure +

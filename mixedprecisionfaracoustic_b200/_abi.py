@@ -84,6 +84,12 @@ _SIGS = [
     ("bp_field_energy", C.c_int, [C.c_void_p, DoubleP]),
     ("bp_get_scaling", C.c_int, [C.c_void_p, IntP, IntP, FloatP, DoubleP, DoubleP]),
     ("bp_write_reference_outputs", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("bp_write_binary_outputs", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("bp_receiver_map", C.c_int, [C.c_void_p, IntP, IntP]),
+    ("bp_copy_traces_async", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, FloatP]),
+    ("bp_checkpoint_size", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    ("bp_checkpoint", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    ("bp_restore", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     ("bp_profile_phases", C.c_int, [C.c_void_p, C.c_int, FloatP]),
     ("bp_algorithmic_bytes", C.c_int, [C.c_void_p, DoubleP, C.POINTER(C.c_longlong)]),
     ("bp_launches_per_step", C.c_int, [C.c_void_p, IntP]),

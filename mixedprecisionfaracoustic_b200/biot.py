@@ -278,6 +278,36 @@ class Simulation:
     def write_reference_outputs(self, directory: str) -> None:
         check(self.lib.bp_write_reference_outputs(self.h, str(directory).encode()), "bp_write_reference_outputs")
 
+    def write_binary_outputs(self, directory: str) -> None:
+        check(self.lib.bp_write_binary_outputs(self.h, str(directory).encode()), "bp_write_binary_outputs")
+
+    def receiver_map(self) -> tuple:
+        """(number of distinct receiver cells, distinct-cell index of each receiver)."""
+        n = C.c_int()
+        m = np.zeros(self.cfg.nrec, dtype=np.int32)
+        check(self.lib.bp_receiver_map(self.h, C.byref(n), _abi.iptr(m)), "bp_receiver_map")
+        return n.value, m
+
+    def copy_traces_async(self, comp, it0: int, out: np.ndarray) -> None:
+        """Enqueues the copy of steps [it0, it0 + out.shape[1]) of one component for
+        every distinct receiver cell into out (float32 [nurec, n], C order); sync() waits."""
+        ci = _abi.TRACE[comp] if isinstance(comp, str) else int(comp)
+        assert out.dtype == np.float32 and out.flags.c_contiguous and out.ndim == 2
+        check(self.lib.bp_copy_traces_async(self.h, ci, int(it0), int(out.shape[1]), _abi.fptr(out)),
+              "bp_copy_traces_async")
+
+    def checkpoint(self) -> bytes:
+        """Image of the evolving state (fields, CPML memory, traces, snapshots, step)."""
+        n = C.c_size_t()
+        check(self.lib.bp_checkpoint_size(self.h, C.byref(n)), "bp_checkpoint_size")
+        buf = (C.c_char * n.value)()
+        check(self.lib.bp_checkpoint(self.h, buf, n.value), "bp_checkpoint")
+        return bytes(buf)
+
+    def restore(self, image: bytes) -> None:
+        buf = C.create_string_buffer(image, len(image))
+        check(self.lib.bp_restore(self.h, buf, len(image)), "bp_restore")
+
 
 class Batch:
     """Many shots advanced by the same launches (bp_batch)."""

@@ -418,6 +418,32 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     return BP_OK;
 }
 
+std::vector<std::pair<void*, size_t>> Shot::state_regions() const {
+    std::vector<std::pair<void*, size_t>> r;
+    const int dim = cfg.dim, prec = cfg.precision;
+    const size_t ncell = (size_t)desc.pitch * desc.ny * desc.nz;
+    const size_t fe = prec == BP_PREC_FP64 ? 8 : (prec == BP_PREC_FP32 ? 4 : 2);
+    const size_t re = prec == BP_PREC_FP64 ? 8 : 4;
+    const size_t ns = dim == 3 ? 4 : 3;
+    for (int f = 0; f < BP_NFIELDS; f++) {
+        if (!field_used(dim, f)) continue;
+        r.emplace_back(desc.f[f], ncell * fe);
+        if (prec == BP_PREC_COMP16) r.emplace_back(desc.flo[f], ncell);
+    }
+    for (int a = 0; a < 3; a++) {
+        if (!desc.psiV[a]) continue;
+        r.emplace_back(desc.psiV[a], 2 * ns * (size_t)desc.slab_cells[a] * re);
+        r.emplace_back(desc.psiT[a], 2 * ns * (size_t)desc.slab_cells[a] * re);
+    }
+    const size_t tr = (size_t)BP_NTRACE * nurec * cfg.nt;
+    r.emplace_back(desc.traces, tr * 4);
+    if (desc.traces64) r.emplace_back(desc.traces64, tr * 8);
+    size_t ncapt = 0;
+    for (long long o : snap_off) ncapt += o >= 0;
+    if (ncapt) r.emplace_back(d_snap, ncapt * snap_n * 4);
+    return r;
+}
+
 void Shot::destroy() {
     if (arena) cudaFree(arena);
     arena = nullptr;

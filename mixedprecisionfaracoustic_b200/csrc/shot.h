@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -78,6 +79,12 @@ struct Shot {
     long long ntiles = 0;              // tiles of the register kernels (128 x 8)
     long long ntiles_s = 0;            // tiles of the TMA-staged 2D kernels (256 x staged_tile_rows)
     long long ntiles_m = 0;            // tasks of the marching 2D kernels (128 cells x zseg_m rows)
+
+    // The device regions that make up the shot's evolving state, in a fixed
+    // order: wavefields (and COMP16 residuals), CPML memory variables of both
+    // phases, recorded traces, captured snapshots.  Everything else in the
+    // arena is fixed by the configuration and medium.
+    std::vector<std::pair<void*, size_t>> state_regions() const;
 
     // Computes the arena size for cfg without allocating (admission control).
     static int plan_bytes(const bp_config* cfg, size_t* bytes);

@@ -31,6 +31,23 @@ struct bp_sim {
         }                                                                                  \
     } while (0)
 
+// Checkpoint image: this header, then the shot's state regions in the order
+// Shot::state_regions lists them.
+struct CkptHeader {
+    char magic[8];
+    int32_t version, precision, dim, order, nx, ny, nz, nt, nurec, it, nregions, pad;
+    uint64_t payload;
+};
+static const char kCkptMagic[8] = {'B', 'P', 'C', 'K', 'P', 'T', '0', '1'};
+
+// Binary output file: this header, then the float32 array, little-endian,
+// last dimension fastest.
+struct BinHeader {
+    char magic[8];
+    int32_t version, dtype, ndims, dims[3];
+};
+static const char kBinMagic[8] = {'B', 'P', 'B', 'I', 'N', '0', '0', '1'};
+
 static const char* kFieldNames[BP_NFIELDS] = {"vux", "vuy", "vuz", "vwx", "vwy", "vwz", "p",
                                               "txx", "tyy", "tzz", "txy", "txz", "tyz"};
 
@@ -199,6 +216,97 @@ int bp_get_traces(bp_sim* s, int comp, float* host, size_t n) {
     if (!u.empty())
         SIM_CK(cudaMemcpy(u.data(), sh.desc.traces + (size_t)comp * sh.nurec * nt, u.size() * 4, cudaMemcpyDeviceToHost));
     for (size_t r = 0; r < nr; r++) std::memcpy(host + r * nt, u.data() + (size_t)sh.urec_of[r] * nt, nt * 4);
+    return BP_OK;
+}
+
+int bp_receiver_map(bp_sim* s, int* nurec, int* map) {
+    if (!s || !nurec) { set_error("bad arguments"); return BP_ERR_ARG; }
+    *nurec = s->shot.nurec;
+    if (map) for (int r = 0; r < s->shot.cfg.nrec; r++) map[r] = s->shot.urec_of[r];
+    return BP_OK;
+}
+
+int bp_copy_traces_async(bp_sim* s, int comp, int it0, int n, float* host) {
+    if (!s || !host || comp < 0 || comp >= BP_NTRACE || it0 < 0 || n < 0 || it0 + n > s->shot.cfg.nt) {
+        set_error("bad arguments");
+        return BP_ERR_ARG;
+    }
+    Shot& sh = s->shot;
+    if (n == 0 || sh.nurec == 0) return BP_OK;
+    const size_t nt = sh.cfg.nt;
+    SIM_CK(cudaSetDevice(s->device));
+    SIM_CK(cudaMemcpy2DAsync(host, (size_t)n * 4, sh.desc.traces + (size_t)comp * sh.nurec * nt + it0, nt * 4,
+                             (size_t)n * 4, sh.nurec, cudaMemcpyDeviceToHost, s->st));
+    return BP_OK;
+}
+
+int bp_checkpoint_size(bp_sim* s, size_t* bytes) {
+    if (!s || !bytes) { set_error("bad arguments"); return BP_ERR_ARG; }
+    size_t n = sizeof(CkptHeader);
+    for (auto& r : s->shot.state_regions()) n += r.second;
+    *bytes = n;
+    return BP_OK;
+}
+
+static void ckpt_header(bp_sim* s, CkptHeader& h) {
+    const Shot& sh = s->shot;
+    std::memset(&h, 0, sizeof h);
+    std::memcpy(h.magic, kCkptMagic, 8);
+    h.version = 1;
+    h.precision = sh.cfg.precision; h.dim = sh.cfg.dim; h.order = sh.cfg.order;
+    h.nx = sh.desc.nx; h.ny = sh.desc.ny; h.nz = sh.desc.nz; h.nt = sh.cfg.nt; h.nurec = sh.nurec;
+    h.it = sh.it_host;
+    const auto regs = sh.state_regions();
+    h.nregions = (int)regs.size();
+    for (auto& r : regs) h.payload += r.second;
+}
+
+int bp_checkpoint(bp_sim* s, void* host, size_t bytes) {
+    if (!s || !host) { set_error("bad arguments"); return BP_ERR_ARG; }
+    size_t need = 0;
+    bp_checkpoint_size(s, &need);
+    if (bytes < need) { set_error("checkpoint buffer too small"); return BP_ERR_ARG; }
+    SIM_CK(cudaSetDevice(s->device));
+    SIM_CK(cudaStreamSynchronize(s->st));
+    int rc = s->run.device_error();
+    if (rc) { set_error("a phase kernel recorded an error"); return rc; }
+    CkptHeader h;
+    ckpt_header(s, h);
+    std::memcpy(host, &h, sizeof h);
+    char* p = static_cast<char*>(host) + sizeof h;
+    for (auto& r : s->shot.state_regions()) {
+        SIM_CK(cudaMemcpyAsync(p, r.first, r.second, cudaMemcpyDeviceToHost, s->st));
+        p += r.second;
+    }
+    SIM_CK(cudaStreamSynchronize(s->st));
+    return BP_OK;
+}
+
+int bp_restore(bp_sim* s, const void* host, size_t bytes) {
+    if (!s || !host || bytes < sizeof(CkptHeader)) { set_error("bad arguments"); return BP_ERR_ARG; }
+    CkptHeader h, mine;
+    std::memcpy(&h, host, sizeof h);
+    ckpt_header(s, mine);
+    if (std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1) { set_error("not a checkpoint image"); return BP_ERR_ARG; }
+    if (h.precision != mine.precision || h.dim != mine.dim || h.order != mine.order || h.nx != mine.nx ||
+        h.ny != mine.ny || h.nz != mine.nz || h.nt != mine.nt || h.nurec != mine.nurec ||
+        h.nregions != mine.nregions || h.payload != mine.payload) {
+        set_error("checkpoint was taken from a simulation of another configuration");
+        return BP_ERR_ARG;
+    }
+    if (bytes < sizeof h + h.payload) { set_error("checkpoint image truncated"); return BP_ERR_ARG; }
+    if (h.it < 0 || h.it > h.nt) { set_error("checkpoint step out of range"); return BP_ERR_ARG; }
+    SIM_CK(cudaSetDevice(s->device));
+    SIM_CK(cudaStreamSynchronize(s->st));
+    const char* p = static_cast<const char*>(host) + sizeof h;
+    for (auto& r : s->shot.state_regions()) {
+        SIM_CK(cudaMemcpyAsync(r.first, p, r.second, cudaMemcpyHostToDevice, s->st));
+        p += r.second;
+    }
+    const int it = h.it;
+    SIM_CK(cudaMemcpyAsync(s->shot.desc.step_base, &it, sizeof(int), cudaMemcpyHostToDevice, s->st));
+    SIM_CK(cudaStreamSynchronize(s->st));
+    s->shot.it_host = it;
     return BP_OK;
 }
 
@@ -411,6 +519,54 @@ static int write_rows(const std::string& path, const float* data, int nr, int nc
         fprintf(fp, "\n");
     }
     fclose(fp);
+    return BP_OK;
+}
+
+static int write_bin(const std::string& path, const float* data, int ndims, const int* dims) {
+    BinHeader h;
+    std::memset(&h, 0, sizeof h);
+    std::memcpy(h.magic, kBinMagic, 8);
+    h.version = 1;
+    h.dtype = 0;
+    h.ndims = ndims;
+    size_t n = 1;
+    for (int i = 0; i < ndims; i++) { h.dims[i] = dims[i]; n *= (size_t)dims[i]; }
+    FILE* fp = fopen(path.c_str(), "wb");
+    if (!fp) { set_error("cannot open " + path); return BP_ERR_ARG; }
+    bool ok = fwrite(&h, sizeof h, 1, fp) == 1 && (n == 0 || fwrite(data, 4, n, fp) == n);
+    ok = (fclose(fp) == 0) && ok;
+    if (!ok) { set_error("short write to " + path); return BP_ERR_ARG; }
+    return BP_OK;
+}
+
+int bp_write_binary_outputs(bp_sim* s, const char* dir) {
+    if (!s || !dir) { set_error("bad arguments"); return BP_ERR_ARG; }
+    mkdir(dir, 0755);
+    Shot& sh = s->shot;
+    const int nt = sh.cfg.nt, nr = sh.cfg.nrec;
+    const std::string d(dir);
+    std::vector<float> all((size_t)BP_NTRACE * nr * nt);
+    for (int c = 0; c < BP_NTRACE; c++) {
+        int rc = bp_get_traces(s, c, all.data() + (size_t)c * nr * nt, (size_t)nr * nt);
+        if (rc) return rc;
+    }
+    const int tdims[3] = {BP_NTRACE, nr, nt};
+    int rc = write_bin(d + "/traces.bin", all.data(), 3, tdims);
+    if (rc) return rc;
+    const int nx = sh.desc.nx, ny = sh.desc.ny, nz = sh.desc.nz;
+    const bool vol = sh.cfg.dim == 3 && sh.cfg.snap_y < 0;
+    std::vector<float> snap(sh.snap_n);
+    for (int k = 0; k < (int)sh.snap_steps.size(); k++) {
+        for (int f = 0; f < BP_NFIELDS; f++) {
+            if (sh.snap_off[(size_t)k * BP_NFIELDS + f] < 0) continue;
+            rc = bp_get_snapshot(s, k, f, snap.data(), snap.size());
+            if (rc) return rc;
+            const int d3[3] = {nz, ny, nx}, d2[2] = {nz, nx};
+            rc = vol ? write_bin(d + "/" + kFieldNames[f] + std::to_string(sh.snap_steps[k]) + ".bin", snap.data(), 3, d3)
+                     : write_bin(d + "/" + kFieldNames[f] + std::to_string(sh.snap_steps[k]) + ".bin", snap.data(), 2, d2);
+            if (rc) return rc;
+        }
+    }
     return BP_OK;
 }
 
