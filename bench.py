@@ -52,8 +52,10 @@ def parse():
     ap.add_argument("--nz", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=20)
-    ap.add_argument("--workload", choices=["c1", "c3", "c4"], default="c1",
-                    help="c1: one 2D shot (default, the headline); c3: 64 batched 2D shots; c4: serving stream")
+    ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4"], default="c1",
+                    help="c1: one 2D shot (default, the headline); c2: one 3D 512x512x384 shot; "
+                         "c3: 64 batched 2D shots; c4: serving stream")
+    ap.add_argument("--crop-steps", type=int, default=1000, help="c2: steps of the 128^3 crop accuracy runs")
     ap.add_argument("--scale", type=float, default=1.0, help="c3/c4: linear size scale of every shot")
     ap.add_argument("--requests", type=int, default=200, help="c4: number of requests")
     ap.add_argument("--precision", choices=["fp32", "comp16"], default="fp32", help="c3/c4 precision")
@@ -342,6 +344,64 @@ def run_batch(args, rank, ws):
             "clocks": clk.summary(), "timing": "host wall clock around bp_batch_run + bp_batch_sync"}
 
 
+def run_c2(args):
+    """c2: the 3D 512x512x384 log-normal model (+20-cell CPML), COMP16 and FP32:
+    Mcell-updates/s and the phase kernels' HBM GB/s against the measured peak;
+    seismogram rel-L2 of COMP16 (and FP32) vs FP64 on a 128^3 crop of the same
+    model around the source (the full model is too large for an FP64 run)."""
+    import torch
+    from mixedprecisionfaracoustic_b200 import Simulation
+    from mixedprecisionfaracoustic_b200.presets import config2, config2_crop
+    torch.cuda.set_device(0)
+    K, W, P = min(args.steps, 300), max(args.warmup, 3), 5
+    peak, peak_kind = measured_peaks()
+    t0 = time.perf_counter()
+    base, med = config2(precision="comp16", nt=W + K + P)
+    gen_s = time.perf_counter() - t0
+    res = {}
+    for prec in ("comp16", "fp32"):
+        base.precision = prec
+        with Simulation(base, med) as s:
+            s.run(W)
+            s.sync()
+            with ClockSampler(0) as clk:
+                ms = s.run_timed(K)
+            (bv, bt), cells = s.algorithmic_bytes()
+            pv, pt, pp = s.profile_phases(P)
+        res[prec] = {"value": cells * K / (ms * 1e-3) / 1e6, "ms_per_step": ms / K,
+                     "phase_ms": {"v_phase": pv, "t_phase": pt, "record_inject": pp},
+                     "hbm_GBps": {"v_phase": bv * cells / (pv * 1e-3) / 1e9, "t_phase": bt * cells / (pt * 1e-3) / 1e9,
+                                  "step": (bv + bt) * cells / ((pv + pt) * 1e-3) / 1e9},
+                     "bytes_per_cell": {"v_phase": bv, "t_phase": bt}, "cells": cells, "clocks": clk.summary()}
+        for k in ("v_phase", "t_phase", "step"):
+            res[prec].setdefault("frac", {})[k] = res[prec]["hbm_GBps"][k] / peak
+    # accuracy on the crop
+    acc = {}
+    ref = None
+    for prec in ("fp64", "comp16", "fp32"):
+        c, m = config2_crop(base, med, size=128, precision=prec, nt=args.crop_steps)
+        s = Simulation(c, m)
+        s.run(c.nt)
+        s.sync()
+        if prec == "fp64":
+            ref = s
+            continue
+        acc[prec] = {comp: s.trace_rel_l2(ref, comp) for comp in ("txx", "tzz", "vux", "p")}
+        s.close()
+    ref.close()
+    c16 = res["comp16"]
+    return {"metric": METRIC, "value": c16["value"], "unit": METRIC, "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": c16["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f16+i8 storage, f32 math", "data": "synthetic",
+            "config": {"workload": "c2: 3D log-normal 512x512x384 (+20-cell CPML = 552x552x424), order 2, "
+                                   "65,536 surface receivers", "medium_generation_s": gen_s,
+                       "l2_flush": "inputs larger than L2"},
+            "roofline": {"bound": "hbm", "kernel": "step", "achieved": c16["hbm_GBps"]["step"], "peak": peak,
+                         "unit": "GB/s", "frac": c16["frac"]["step"], "peak_source": peak_kind},
+            "comp16": c16, "fp32": res["fp32"], "speedup_comp16_vs_fp32": c16["value"] / res["fp32"]["value"],
+            "rel_l2_vs_fp64_crop128": {"steps": args.crop_steps, **acc}}
+
+
 def run_serve(args, rank):
     """c4: Poisson stream of shot requests into the server at ~80% of its measured
     capacity; p50/p99 latency and Mcell-updates/s (rank 0 only)."""
@@ -392,6 +452,10 @@ def run_serve(args, rank):
 def main():
     args = parse()
     ws, rank, local = dist_env()
+    if args.workload == "c2" and args.impl == "ours":
+        if rank == 0:
+            print(json.dumps(run_c2(args)), flush=True)
+        return 0
     if args.workload != "c1" and args.impl == "ours":
         if ws > 1:
             import torch

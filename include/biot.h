@@ -282,6 +282,15 @@ int bp_trace_rel_l2(bp_sim* x, bp_sim* ref, int comp, double* rel);
 
 void bp_destroy(bp_sim* sim);
 
+/* Device memory of destroyed simulations, batches and served requests is kept
+ * per device for reuse by the next one of a similar size (no counterpart in
+ * the reference, which allocates once): a cudaFree of a GB-size block costs
+ * 0.4-1 s.  The cache holds at most a quarter of the device's memory (32 GiB
+ * at most; environment variable BP_ARENA_CACHE_MB overrides, 0 disables) and
+ * is emptied when an allocation fails.  This call returns it to the system
+ * for one device, or for all with device = -1. */
+int bp_release_cached_memory(int device);
+
 const char* bp_error_string(int code);
 const char* bp_last_error(void);
 

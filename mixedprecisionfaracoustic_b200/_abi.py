@@ -100,6 +100,7 @@ _SIGS = [
     ("bp_rel_l2_device_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, DoubleP]),
     ("bp_trace_rel_l2", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, DoubleP]),
     ("bp_destroy", None, [C.c_void_p]),
+    ("bp_release_cached_memory", C.c_int, [C.c_int]),
     ("bp_error_string", C.c_char_p, [C.c_int]),
     ("bp_last_error", C.c_char_p, []),
     ("bp_medium_reference_borehole", C.c_int, [C.c_int, C.c_int, C.c_int, FloatP]),

@@ -6,10 +6,14 @@
 //   tables, slab-only CPML memory variables, the source wavelet, receiver
 //   indices, trace and snapshot buffers, reduction scratch and the device copy
 //   of the shot descriptor.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include "shot.h"
 
@@ -252,7 +256,7 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     Plan p;
     make_plan(&cfg, nurec, p);
     arena_bytes = p.total;
-    BP_CK(cudaMalloc(&arena, arena_bytes));
+    BP_CK(arena_alloc(arena_bytes, &arena, &arena_alloc_bytes));
     BP_CK(cudaMemsetAsync(arena, 0, arena_bytes, st));
     char* A = static_cast<char*>(arena);
     auto at = [&](size_t o) -> void* { return o == (size_t)-1 ? nullptr : (void*)(A + o); };
@@ -444,8 +448,118 @@ std::vector<std::pair<void*, size_t>> Shot::state_regions() const {
     return r;
 }
 
+// ---- arena cache --------------------------------------------------------
+// A destroyed shot's arena is kept for the next shot of a similar size on the
+// same device instead of being returned with cudaFree, whose cost for a GB-size
+// block (0.4-1 s measured on B200) would dominate short runs and the
+// create/destroy churn of the serving loop.  Bounded per device (a quarter of
+// its memory, at most 32 GiB; BP_ARENA_CACHE_MB overrides, 0 disables);
+// emptied when an allocation fails, and by bp_release_cached_memory.
+namespace {
+struct CachedArena {
+    int device;
+    void* ptr;
+    size_t bytes;
+};
+std::mutex g_arena_mu;
+std::vector<CachedArena> g_arenas;
+
+size_t arena_cache_limit(int device) {
+    static long long env = -2;
+    if (env == -2) {
+        const char* v = getenv("BP_ARENA_CACHE_MB");
+        env = v ? atoll(v) : -1;
+    }
+    if (env >= 0) return (size_t)env << 20;
+    size_t total = 0, freeb = 0;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != device) return 0;
+    if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return std::min(total / 4, (size_t)32 << 30);
+}
+
+void free_cached(int device) {   // g_arena_mu held; device -1 = all devices
+    int cur = -1;
+    cudaGetDevice(&cur);
+    for (size_t i = 0; i < g_arenas.size();) {
+        if (device < 0 || g_arenas[i].device == device) {
+            if (g_arenas[i].device != cur) cudaSetDevice(g_arenas[i].device);
+            cudaFree(g_arenas[i].ptr);
+            g_arenas.erase(g_arenas.begin() + i);
+        } else {
+            i++;
+        }
+    }
+    if (cur >= 0) cudaSetDevice(cur);
+}
+}  // namespace
+
+// An arena of at least `bytes` on the current device: a cached one of up to
+// 1.25x that size, else a new allocation (after emptying this device's cache
+// if the first attempt fails).  *got is the block's real size.
+cudaError_t arena_alloc(size_t bytes, void** ptr, size_t* got) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> g(g_arena_mu);
+        int best = -1;
+        for (int i = 0; i < (int)g_arenas.size(); i++) {
+            const CachedArena& a = g_arenas[i];
+            if (a.device == dev && a.bytes >= bytes && a.bytes <= bytes + bytes / 4 &&
+                (best < 0 || a.bytes < g_arenas[best].bytes))
+                best = i;
+        }
+        if (best >= 0) {
+            *ptr = g_arenas[best].ptr;
+            *got = g_arenas[best].bytes;
+            g_arenas.erase(g_arenas.begin() + best);
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        {
+            std::lock_guard<std::mutex> g(g_arena_mu);
+            free_cached(dev);
+        }
+        e = cudaMalloc(ptr, bytes);
+    }
+    if (e == cudaSuccess) *got = bytes;
+    return e;
+}
+
+void arena_release(void* ptr, size_t bytes) {
+    if (!ptr) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t limit = arena_cache_limit(dev);
+    std::lock_guard<std::mutex> g(g_arena_mu);
+    size_t held = 0;
+    for (const CachedArena& a : g_arenas)
+        if (a.device == dev) held += a.bytes;
+    // evict the oldest entries of this device until the block fits
+    for (size_t i = 0; held + bytes > limit && i < g_arenas.size();) {
+        if (g_arenas[i].device == dev) {
+            held -= g_arenas[i].bytes;
+            cudaFree(g_arenas[i].ptr);
+            g_arenas.erase(g_arenas.begin() + i);
+        } else {
+            i++;
+        }
+    }
+    if (held + bytes <= limit) g_arenas.push_back({dev, ptr, bytes});
+    else cudaFree(ptr);
+}
+
+void release_cached_arenas(int device) {
+    std::lock_guard<std::mutex> g(g_arena_mu);
+    free_cached(device);
+}
+
 void Shot::destroy() {
-    if (arena) cudaFree(arena);
+    if (arena) arena_release(arena, arena_alloc_bytes);
     arena = nullptr;
 }
 

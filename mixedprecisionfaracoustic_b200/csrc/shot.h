@@ -56,6 +56,11 @@ cudaError_t launch_rel_l2(const float* x, const float* ref, long long n, double*
 
 void set_error(const std::string& msg);
 
+// Arena blocks: reused across shots on a device (see shot.cu).
+cudaError_t arena_alloc(size_t bytes, void** ptr, size_t* got);
+void arena_release(void* ptr, size_t bytes);
+void release_cached_arenas(int device);   // -1: every device
+
 struct Shot {
     bp_config cfg{};
     std::vector<int> rec_x, rec_y, rec_z, snap_steps;
@@ -65,7 +70,8 @@ struct Shot {
     ShotDesc desc{};                   // host copy of the device descriptor
     ShotDesc* d_desc = nullptr;        // device copy (single-shot runs)
     void* arena = nullptr;
-    size_t arena_bytes = 0;
+    size_t arena_bytes = 0;            // bytes the plan uses
+    size_t arena_alloc_bytes = 0;      // size of the block (a reused cached block may be larger)
     int em = 0, es = 0;
     double kmax = 0, rmax = 0;
     std::vector<float> dyn;            // COMP16 state scale per step

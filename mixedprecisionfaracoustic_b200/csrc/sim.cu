@@ -219,6 +219,12 @@ int bp_get_traces(bp_sim* s, int comp, float* host, size_t n) {
     return BP_OK;
 }
 
+int bp_release_cached_memory(int device) {
+    if (device < -1) { set_error("bad device"); return BP_ERR_ARG; }
+    release_cached_arenas(device);
+    return BP_OK;
+}
+
 int bp_receiver_map(bp_sim* s, int* nurec, int* map) {
     if (!s || !nurec) { set_error("bad arguments"); return BP_ERR_ARG; }
     *nurec = s->shot.nurec;

@@ -195,6 +195,28 @@ def config2(precision: str = "comp16", seed: int = 2, n=(512, 512, 384), npml: i
     return cfg, med
 
 
+def config2_crop(cfg, med, size: int = 128, precision: str = "fp64", nt: int = None):
+    """A size^3 crop of a c2 model: the top `size` cells in depth of the size x size
+    columns centred on the source, the same medium values cell for cell, the same
+    source cell and the surface receivers that fall inside the crop."""
+    nx, ny, nz, np_ = cfg.nx, cfg.ny, cfg.nz, cfg.npml
+    sx, sy, sz = (c - np_ for c in cfg.src)            # physical source cell
+    x0 = min(max(sx - size // 2, 0), nx - size)
+    y0 = min(max(sy - size // 2, 0), ny - size)
+    z0 = 0
+    sl = (slice(z0, z0 + size), slice(y0, y0 + size), slice(x0, x0 + size))
+    cm = Medium({k: np.ascontiguousarray(np.asarray(v).reshape(nz, ny, nx)[sl]) for k, v in med.items()})
+    keep = [i for i in range(cfg.nrec)
+            if x0 <= cfg.rec_x[i] - np_ < x0 + size and y0 <= cfg.rec_y[i] - np_ < y0 + size
+            and z0 <= cfg.rec_z[i] - np_ < z0 + size]
+    out = ShotConfig(dim=3, nx=size, ny=size, nz=size, npml=np_, order=cfg.order, precision=precision,
+                     nt=cfg.nt if nt is None else nt, dx=cfg.dx, dt=cfg.dt, f0=cfg.f0, pml_v0=cfg.pml_v0,
+                     pml_r=cfg.pml_r, src=(np_ + sx - x0, np_ + sy - y0, np_ + sz - z0), src_mask=cfg.src_mask,
+                     rec_x=[cfg.rec_x[i] - x0 for i in keep], rec_y=[cfg.rec_y[i] - y0 for i in keep],
+                     rec_z=[cfg.rec_z[i] - z0 for i in keep], check_cfl=cfg.check_cfl)
+    return out, cm
+
+
 def config3_shots(seed: int = 3, nshots: int = 64, nt: int = 4000, precision: str = "fp32", npml: int = 20,
                   sizes=((1024, 1024), (1536, 1024), (2048, 2048), (3072, 1536)), order: int = 2,
                   scale: float = 1.0):

@@ -35,6 +35,18 @@ def test_config0_and_2():
     assert cfg2.dt < cfl_limit(cfg2, med2)[0]
 
 
+def test_config2_crop_is_a_crop():
+    from mixedprecisionfaracoustic_b200.presets import config2_crop
+    cfg, med = config2(n=(40, 36, 32), nrec_side=8, nt=10)
+    c, m = config2_crop(cfg, med, size=16)
+    assert c.padded == (56, 56, 56) and c.precision == "fp64"
+    x0, y0 = 20 - 8, 18 - 8                              # columns centred on the source (20, 18)
+    full = np.asarray(med["H"]).reshape(32, 36, 40)
+    assert np.array_equal(np.asarray(m["H"]).reshape(16, 16, 16), full[:16, y0:y0 + 16, x0:x0 + 16])
+    assert c.src == (cfg.npml + 8, cfg.npml + 8, cfg.npml + 1)
+    assert c.nrec > 0 and all(cfg.npml <= x < cfg.npml + 16 for x in c.rec_x)
+
+
 def test_lognormal_statistics():
     rng = np.random.default_rng(2)
     f = lognormal_field((48, 64, 64), 0.1, 10.0, rng)
