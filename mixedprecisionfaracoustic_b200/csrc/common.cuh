@@ -104,44 +104,32 @@ struct ShotDesc {
 // ---------------------------------------------------------------------------
 // Compensated FP16 codec (the reference's store_ch / load_ch,
 // Half/main.cu:59-100): value ~ hi + lo * u(hi), u = fp16 ulp(hi) / 256
-// = 2^(e-19) with e the frexp exponent of |hi|, and u = 2^-32 for |hi| < 2^-14.
-// The exponent is taken from the fp32 bit pattern (exact, same as frexpf).
-__device__ __forceinline__ float residual_unit(float hi) {
-    float a = fabsf(hi);
-    if (a < 6.103515625e-5f) return 2.3283064365386963e-10f;
-    unsigned u = __float_as_uint(a);
-    int e = (int)((u >> 23) & 0xff) - 126;   // frexpf exponent: a = m * 2^e, m in [0.5,1)
-    return __uint_as_float((unsigned)(e - 19 + 127) << 23);
-}
-// The same unit from the fp16 bits: for biased exponent E of hi, frexp gives
-// e = E - 14 (normal) and |hi| < 2^-14 exactly when E <= 1 with 2^(1-33) =
-// 2^-32, so u = 2^(max(E, 1) - 33): float bits (max(E, 1) + 94) << 23.
-__device__ __forceinline__ float unit_from_half_bits(unsigned hb) {
-    unsigned E = (hb >> 10) & 31u;
-    E = E > 1u ? E : 1u;
-    return __uint_as_float((E + 94u) << 23);
-}
-__device__ __forceinline__ float unit_inv_from_half_bits(unsigned hb) {
-    unsigned E = (hb >> 10) & 31u;
-    E = E > 1u ? E : 1u;
-    return __uint_as_float((160u - E) << 23);
+// = 2^(e-19) with e the frexp exponent of |hi|, and u = 2^-32 for |hi| < 2^-14;
+// for the biased fp16 exponent E of hi that is u = 2^(max(E, 1) - 33).
+//
+// Both directions work from the float value of hi: its exponent field masked
+// out, m = 2^(E-15) for a normal hi, is clamped below to 2^-14 (zero and
+// subnormal hi, E = 0) and above to 2^15 (inf / NaN hi, where the scale only
+// has to stay finite), so u = 2^-18 m and 1/u = 2^18 / m are exact powers of
+// two formed by integer operations on the float bits.  Checked bit for bit
+// against the direct exponent-field form over all 2^24 (hi, lo) pairs and all
+// 2^32 float inputs; this form takes 6 instead of 9 instructions per decode.
+__device__ __forceinline__ unsigned half_scale_bits(float hf) {
+    unsigned m = __float_as_uint(hf) & 0x7f800000u;
+    m = m > 0x38800000u ? m : 0x38800000u;
+    return m < 0x47000000u ? m : 0x47000000u;
 }
 __device__ __forceinline__ float decode_ch(__half hi, int8_t lo) {
-    return __half2float(hi) + (float)lo * unit_from_half_bits(__half_as_ushort(hi));
-}
-// 1 / residual_unit(hi), also an exact power of two, so the quotient of the
-// reference's (v - hi) / u is formed exactly by a multiplication.
-__device__ __forceinline__ float residual_unit_inv(float hi) {
-    float a = fabsf(hi);
-    if (a < 6.103515625e-5f) return 4294967296.0f;
-    unsigned u = __float_as_uint(a);
-    int e = (int)((u >> 23) & 0xff) - 126;
-    return __uint_as_float((unsigned)(19 - e + 127) << 23);
+    const float hf = __half2float(hi);
+    // lo * 2^-18, exact: the int8 added to the bits of 48.0f (ulp 2^-18) minus 48
+    const float lof = __int_as_float(0x42400000 + (int)lo) - 48.0f;
+    return fmaf(lof, __uint_as_float(half_scale_bits(hf)), hf);   // hi + lo u, exact
 }
 __device__ __forceinline__ void encode_ch(float v, __half& hi, int8_t& lo) {
-    __half h = __float2half_rn(v);
-    float hf = __half2float(h);
-    float scaled = (v - hf) * unit_inv_from_half_bits(__half_as_ushort(h));
+    const __half h = __float2half_rn(v);
+    const float hf = __half2float(h);
+    const float uinv = __uint_as_float(0x88000000u - half_scale_bits(hf));   // 1/u = 2^18 / m
+    const float scaled = (v - hf) * uinv;                                      // exact
     int q = __float2int_rz(scaled + copysignf(0.5f, scaled));   // round half away from zero
     q = q > 127 ? 127 : (q < -127 ? -127 : q);
     hi = h;

@@ -37,21 +37,22 @@ __device__ __forceinline__ int locate_shot(const ShotDesc* shots, int nshots, lo
 // Resident CTAs per SM the 2D FP32/COMP16 phase kernels are register-limited
 // to (1 = no limit).  Measured on B200 for the 4040 x 2040 order-2 grid: FP32
 // is fastest at 3 (80 registers, no spills); COMP16, whose decode/encode
-// chains leave it latency-bound, at 4 (64 registers, a few spilled values).
+// chains leave it latency-bound, at 5 (48 registers, some spilled values).
 #ifndef BP_MINB_F32
 #define BP_MINB_F32 3
 #endif
 #ifndef BP_MINB_C16
-#define BP_MINB_C16 4
+#define BP_MINB_C16 5
 #endif
 // 3D: uncapped, the kernels take 128-169 registers (1-2 CTAs per SM); capped
 // at 3 CTAs (80 registers, ~150 bytes spilled) the 192^3 order-2 and 200^3
-// order-4 steps run 1.75-2.1x faster on B200, FP32 and COMP16 alike.
+// order-4 steps run 1.75-2.1x faster on B200, FP32 and COMP16 alike.  COMP16
+// gains another 7 % at 4 CTAs on the 552 x 552 x 424 order-2 grid.
 #ifndef BP_MINB3_F32
 #define BP_MINB3_F32 3
 #endif
 #ifndef BP_MINB3_C16
-#define BP_MINB3_C16 3
+#define BP_MINB3_C16 4
 #endif
 template <int DIM, class P, bool VPHASE>
 __host__ __device__ constexpr int phase_min_blocks() {
