@@ -77,21 +77,32 @@ __device__ __forceinline__ void load_rows(const void* p, const int8_t* lo, long 
     for (int k = 0; k <= ORD; k++) P::ld4(p, lo, c + (long long)(k - HW) * stride, a[k]);
 }
 
+// Product by the COMP16 rescale factor, never fused into a neighbouring add:
+// the kernels skip it when the factor is exactly 1 (all steps but one in a
+// hundred), and x * 1 == x only holds if no FMA ever absorbs the product.
+template <class R>
+__device__ __forceinline__ R mulr(R x, R r) {
+    if constexpr (sizeof(R) == 4) return __fmul_rn(x, r);
+    else return __dmul_rn(x, r);
+}
 template <class R>
 __device__ __forceinline__ void scale4(R (&v)[4], R r) {
 #pragma unroll
-    for (int j = 0; j < 4; j++) v[j] *= r;
+    for (int j = 0; j < 4; j++) v[j] = mulr(v[j], r);
 }
 
 // CPML memory update of one derivative slot for a 4-cell chunk
 // (Float/main.cu:130-158):  ψ = ψ e + b (e prev + ∂),  prev = ∂,  ∂ += ψ,
 // with b = -DT d / 2 precomputed.  The x axis has per-cell tables; the y and z
 // axes one value per chunk.  Old ψ/prev are multiplied by the state rescale r.
-template <class R>
+template <bool RS, class R>
 __device__ __forceinline__ void cpml_x(R (&d)[4], R* psi, R* prev, const R* b, const R* e, int x0, R r) {
     R ps[4], pv[4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) { ps[j] = psi[j] * r; pv[j] = prev[j] * r; }
+    for (int j = 0; j < 4; j++) {
+        ps[j] = RS ? mulr(psi[j], r) : psi[j];
+        pv[j] = RS ? mulr(prev[j], r) : prev[j];
+    }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         R ee = e[x0 + j], bb = b[x0 + j];
@@ -103,11 +114,14 @@ __device__ __forceinline__ void cpml_x(R (&d)[4], R* psi, R* prev, const R* b, c
 #pragma unroll
     for (int j = 0; j < 4; j++) { psi[j] = ps[j]; prev[j] = pv[j]; }
 }
-template <class R>
+template <bool RS, class R>
 __device__ __forceinline__ void cpml_s(R (&d)[4], R* psi, R* prev, R bb, R ee, R r) {
     R ps[4], pv[4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) { ps[j] = psi[j] * r; pv[j] = prev[j] * r; }
+    for (int j = 0; j < 4; j++) {
+        ps[j] = RS ? mulr(psi[j], r) : psi[j];
+        pv[j] = RS ? mulr(prev[j], r) : prev[j];
+    }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         R np = ps[j] * ee + bb * (ee * pv[j] + d[j]);
@@ -143,7 +157,7 @@ struct PsiIO {
 
 // One derivative slot of one axis: memory variables k (ψ) and NS+k (prev) of
 // the (phase, axis) slab array; fwd selects the half-grid profile.
-template <int NS, class R>
+template <int NS, bool RS, class R>
 __device__ __forceinline__ void cpml_slot(R (&d)[4], void* base, long long cells, int k, long long sidx,
                                           bool xaxis, int pos, int x0, const void* pb, const void* pe, R r) {
     R* ps = static_cast<R*>(base) + (long long)k * cells + sidx;
@@ -153,8 +167,8 @@ __device__ __forceinline__ void cpml_slot(R (&d)[4], void* base, long long cells
     PsiIO<R>::ld(pv, pvv);
     const R* b = static_cast<const R*>(pb);
     const R* e = static_cast<const R*>(pe);
-    if (xaxis) cpml_x<R>(d, psv, pvv, b, e, x0, r);
-    else cpml_s<R>(d, psv, pvv, b[pos], e[pos], r);
+    if (xaxis) cpml_x<RS, R>(d, psv, pvv, b, e, x0, r);
+    else cpml_s<RS, R>(d, psv, pvv, b[pos], e[pos], r);
     PsiIO<R>::st(ps, psv);
     PsiIO<R>::st(pv, pvv);
 }
@@ -182,6 +196,8 @@ __device__ __forceinline__ long long slab_index(const ShotDesc& S, int axis, int
 // masking, CPML memory variables, divergence, the velocity updates and their
 // stores.  PRE: the caller has already loaded the coefficients and old
 // velocities into V (the marching kernel); otherwise they are loaded here.
+// RS: old state is multiplied by the COMP16 rescale r; the kernels pass false
+// when r is exactly 1, which gives the same bits without the products.
 template <class R>
 struct VState {
     R x1[4], x3[4], s1[4], z1[4], z2[4], s3[4];       // derivatives (2D and 3D)
@@ -190,7 +206,7 @@ struct VState {
     R rho_y[4], c1_y[4], c2_y[4], vu_y[4], vw_y[4];
 };
 
-template <int DIM, int ORD, class P, bool PRE>
+template <int DIM, int ORD, class P, bool PRE, bool RS>
 __device__ __forceinline__ void v_tail(const ShotDesc& S, long long c, int x0, int y, int z, typename P::real r,
                                        unsigned mask, VState<typename P::real>& V) {
     using R = typename P::real;
@@ -208,7 +224,7 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, long long c, int x0, i
         P::ld4(S.f[fw], S.flo[fw], c, vw);
     };
     // the rescale factor applies to old stresses: scale their derivatives
-    if constexpr (P::prec == BP_PREC_COMP16) {
+    if constexpr (P::prec == BP_PREC_COMP16 && RS) {
         scale4(x1, r); scale4(s1, r); scale4(z2, r); scale4(x3, r); scale4(z1, r); scale4(s3, r);
         if constexpr (DIM == 3) { scale4(x2, r); scale4(y1, r); scale4(y2, r); scale4(y3, r); scale4(s2, r); scale4(z3, r); }
     }
@@ -227,30 +243,30 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, long long c, int x0, i
         if (si >= 0) {
             void* B = S.psiV[0];
             const long long n = S.slab_cells[0];
-            cpml_slot<NS, R>(x1, B, n, 0, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            cpml_slot<NS, R>(s1, B, n, 1, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            cpml_slot<NS, R>(z2, B, n, 2, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            if constexpr (DIM == 3) cpml_slot<NS, R>(y2, B, n, 3, si, true, x0, x0, S.pb[0], S.pe[0], r);
+            cpml_slot<NS, RS, R>(x1, B, n, 0, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
+            cpml_slot<NS, RS, R>(s1, B, n, 1, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
+            cpml_slot<NS, RS, R>(z2, B, n, 2, si, true, x0, x0, S.pb[0], S.pe[0], r);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R>(y2, B, n, 3, si, true, x0, x0, S.pb[0], S.pe[0], r);
         }
         if constexpr (DIM == 3) {
             si = slab_index(S, 1, x0, y, z);
             if (si >= 0) {
                 void* B = S.psiV[1];
                 const long long n = S.slab_cells[1];
-                cpml_slot<NS, R>(x2, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, R>(y1, B, n, 1, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, R>(s2, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, R>(z3, B, n, 3, si, false, y, x0, S.pb[1], S.pe[1], r);
+                cpml_slot<NS, RS, R>(x2, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
+                cpml_slot<NS, RS, R>(y1, B, n, 1, si, false, y, x0, S.pb2[1], S.pe2[1], r);
+                cpml_slot<NS, RS, R>(s2, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
+                cpml_slot<NS, RS, R>(z3, B, n, 3, si, false, y, x0, S.pb[1], S.pe[1], r);
             }
         }
         si = slab_index(S, 2, x0, y, z);
         if (si >= 0) {
             void* B = S.psiV[2];
             const long long n = S.slab_cells[2];
-            cpml_slot<NS, R>(x3, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, R>(z1, B, n, 1, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            cpml_slot<NS, R>(s3, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            if constexpr (DIM == 3) cpml_slot<NS, R>(y3, B, n, 3, si, false, z, x0, S.pb[2], S.pe[2], r);
+            cpml_slot<NS, RS, R>(x3, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
+            cpml_slot<NS, RS, R>(z1, B, n, 1, si, false, z, x0, S.pb2[2], S.pe2[2], r);
+            cpml_slot<NS, RS, R>(s3, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R>(y3, B, n, 3, si, false, z, x0, S.pb[2], S.pe[2], r);
         }
     }
 
@@ -276,7 +292,7 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, long long c, int x0, i
         for (int j = 0; j < 4; j++) {
             if constexpr (P::prec == BP_PREC_COMP16) {
                 // Half/main.cu:256-262 with Bt = (rhof rho^-1) Bp formed here
-                R wo = vw[j] * r, uo = vu[j] * r;
+                const R wo = RS ? mulr(vw[j], r) : vw[j], uo = RS ? mulr(vu[j], r) : vu[j];
                 R rr = rf[j] * rho[j];                    // rhof * rho^-1
                 R wn = c1[j] * wo - (rr * c2[j]) * sum[j] - c2[j] * dp[j];
                 nw[j] = wn;
@@ -323,7 +339,7 @@ struct TState {
     R mxy[4], myz[4], oyy[4], oxy[4], oyz[4];
 };
 
-template <int DIM, int ORD, class P, bool PRE>
+template <int DIM, int ORD, class P, bool PRE, bool RS>
 __device__ __forceinline__ void t_tail(const ShotDesc& S, long long c, int x0, int y, int z, typename P::real r,
                                        unsigned mask, TState<typename P::real>& T) {
     using R = typename P::real;
@@ -349,7 +365,7 @@ __device__ __forceinline__ void t_tail(const ShotDesc& S, long long c, int x0, i
             P::ld4(S.f[BP_F_TXY], S.flo[BP_F_TXY], c, oxy);
             P::ld4(S.f[BP_F_TYZ], S.flo[BP_F_TYZ], c, oyz);
         }
-        if constexpr (P::prec == BP_PREC_COMP16) {     // old state takes this step's rescale
+        if constexpr (P::prec == BP_PREC_COMP16 && RS) {     // old state takes this step's rescale
             scale4(op, r); scale4(oxx, r); scale4(ozz, r); scale4(oxz, r);
             if constexpr (DIM == 3) { scale4(oyy, r); scale4(oxy, r); scale4(oyz, r); }
         }
@@ -369,30 +385,30 @@ __device__ __forceinline__ void t_tail(const ShotDesc& S, long long c, int x0, i
         if (si >= 0) {
             void* B = S.psiT[0];
             const long long n = S.slab_cells[0];
-            cpml_slot<NS, R>(uxx, B, n, 0, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            cpml_slot<NS, R>(wx, B, n, 1, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            cpml_slot<NS, R>(uzx, B, n, 2, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            if constexpr (DIM == 3) cpml_slot<NS, R>(uyx, B, n, 3, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
+            cpml_slot<NS, RS, R>(uxx, B, n, 0, si, true, x0, x0, S.pb[0], S.pe[0], r);
+            cpml_slot<NS, RS, R>(wx, B, n, 1, si, true, x0, x0, S.pb[0], S.pe[0], r);
+            cpml_slot<NS, RS, R>(uzx, B, n, 2, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R>(uyx, B, n, 3, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
         }
         if constexpr (DIM == 3) {
             si = slab_index(S, 1, x0, y, z);
             if (si >= 0) {
                 void* B = S.psiT[1];
                 const long long n = S.slab_cells[1];
-                cpml_slot<NS, R>(uyy, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, R>(wy, B, n, 1, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, R>(uxy, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, R>(uzy, B, n, 3, si, false, y, x0, S.pb2[1], S.pe2[1], r);
+                cpml_slot<NS, RS, R>(uyy, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
+                cpml_slot<NS, RS, R>(wy, B, n, 1, si, false, y, x0, S.pb[1], S.pe[1], r);
+                cpml_slot<NS, RS, R>(uxy, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
+                cpml_slot<NS, RS, R>(uzy, B, n, 3, si, false, y, x0, S.pb2[1], S.pe2[1], r);
             }
         }
         si = slab_index(S, 2, x0, y, z);
         if (si >= 0) {
             void* B = S.psiT[2];
             const long long n = S.slab_cells[2];
-            cpml_slot<NS, R>(uzz, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, R>(wz, B, n, 1, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, R>(uxz, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            if constexpr (DIM == 3) cpml_slot<NS, R>(uyz, B, n, 3, si, false, z, x0, S.pb2[2], S.pe2[2], r);
+            cpml_slot<NS, RS, R>(uzz, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
+            cpml_slot<NS, RS, R>(wz, B, n, 1, si, false, z, x0, S.pb[2], S.pe[2], r);
+            cpml_slot<NS, RS, R>(uxz, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R>(uyz, B, n, 3, si, false, z, x0, S.pb2[2], S.pe2[2], r);
         }
     }
 

@@ -34,15 +34,22 @@ __device__ __forceinline__ int locate_shot(const ShotDesc* shots, int nshots, lo
     return lo;
 }
 
+#ifndef BP_RS_SPLIT
+#define BP_RS_SPLIT 1
+#endif
 // Resident CTAs per SM the 2D FP32/COMP16 phase kernels are register-limited
 // to (1 = no limit).  Measured on B200 for the 4040 x 2040 order-2 grid: FP32
 // is fastest at 3 (80 registers, no spills); COMP16, whose decode/encode
-// chains leave it latency-bound, at 5 (48 registers, some spilled values).
+// chains leave it latency-bound, at 6 for the V phase (40 registers) and 5 for
+// the T phase (48 registers), both with some spilled values.
 #ifndef BP_MINB_F32
 #define BP_MINB_F32 3
 #endif
 #ifndef BP_MINB_C16
 #define BP_MINB_C16 5
+#endif
+#ifndef BP_MINB_C16_V
+#define BP_MINB_C16_V 6
 #endif
 // 3D: uncapped, the kernels take 128-169 registers (1-2 CTAs per SM); capped
 // at 3 CTAs (80 registers, ~150 bytes spilled) the 192^3 order-2 and 200^3
@@ -57,7 +64,8 @@ __device__ __forceinline__ int locate_shot(const ShotDesc* shots, int nshots, lo
 template <int DIM, class P, bool VPHASE>
 __host__ __device__ constexpr int phase_min_blocks() {
     if (DIM == 3) return P::prec == BP_PREC_FP32 ? BP_MINB3_F32 : P::prec == BP_PREC_COMP16 ? BP_MINB3_C16 : 1;
-    return P::prec == BP_PREC_FP32 ? BP_MINB_F32 : P::prec == BP_PREC_COMP16 ? BP_MINB_C16 : 1;
+    return P::prec == BP_PREC_FP32 ? BP_MINB_F32
+                                   : P::prec == BP_PREC_COMP16 ? (VPHASE ? BP_MINB_C16_V : BP_MINB_C16) : 1;
 }
 // How a tile learns its step index: 1 = once per shot per launch, 0 = a read
 // of the step counter per tile (measured faster for FP32 at 80 registers).
@@ -74,7 +82,7 @@ __host__ __device__ constexpr bool step_once_per_shot() {
 
 // ---------------------------------------------------------------------------
 // V phase for one 4-cell chunk: FD_V (Float/main.cu:103-191).
-template <int DIM, int ORD, class P>
+template <int DIM, int ORD, class P, bool RS>
 __device__ __forceinline__ void v_chunk(const ShotDesc& S, int x0, int y, int z, typename P::real r,
                                         unsigned mask) {
     using R = typename P::real;
@@ -153,12 +161,12 @@ __device__ __forceinline__ void v_chunk(const ShotDesc& S, int x0, int y, int z,
                 s2[j] = deriv_div<P>(rfwd<ORD>(t), S); }
         }
     }
-    v_tail<DIM, ORD, P, false>(S, c, x0, y, z, r, mask, V);
+    v_tail<DIM, ORD, P, false, RS>(S, c, x0, y, z, r, mask, V);
 }
 
 // ---------------------------------------------------------------------------
 // T phase for one 4-cell chunk: FD_T (Float/main.cu:232-294).
-template <int DIM, int ORD, class P>
+template <int DIM, int ORD, class P, bool RS>
 __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z, typename P::real r,
                                         unsigned mask) {
     using R = typename P::real;
@@ -236,7 +244,7 @@ __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z,
                 uzy[j] = deriv_div<P>(rfwd<ORD>(t), S); }
         }
     }
-    t_tail<DIM, ORD, P, false>(S, c, x0, y, z, r, mask, T);
+    t_tail<DIM, ORD, P, false, RS>(S, c, x0, y, z, r, mask, T);
 }
 
 // ---------------------------------------------------------------------------
@@ -299,8 +307,16 @@ __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, P, VPHASE>())
 #pragma unroll
         for (int j = 0; j < 4; j++)
             if (x0 + j >= hw && x0 + j < S.nx - hw) mask |= 1u << j;
-        if constexpr (VPHASE) v_chunk<DIM, ORD, P>(S, x0, y, z, r, mask);
-        else t_chunk<DIM, ORD, P>(S, x0, y, z, r, mask);
+        // COMP16: the rescale products only on the steps whose factor is not
+        // exactly 1 (a uniform branch; the products are never fused, so both
+        // forms give the same bits when r == 1)
+        if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
+            if constexpr (VPHASE) v_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+            else t_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+        } else {
+            if constexpr (VPHASE) v_chunk<DIM, ORD, P, false>(S, x0, y, z, r, mask);
+            else t_chunk<DIM, ORD, P, false>(S, x0, y, z, r, mask);
+        }
     }
 }
 

@@ -246,7 +246,10 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
                 V.z1[j] = dz_fwd<ORD, P>(wzz, j, S);                   // tzz: D+z
                 V.s3[j] = dz_fwd<ORD, P>(wp, j, S);                    // p: D+z
             }
-            if (act) v_tail<2, ORD, P, !kLean>(S, c, x0, 0, z, r, mask, V);
+            if (act) {
+                if (P::prec == BP_PREC_COMP16 && r != (R)1) v_tail<2, ORD, P, !kLean, true>(S, c, x0, 0, z, r, mask, V);
+                else v_tail<2, ORD, P, !kLean, false>(S, c, x0, 0, z, r, mask, V);
+            }
             shift(wp);
             shift(wzz);
             shift(wxz);
@@ -308,7 +311,7 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
                 P::dec4(L.cC, T.cC); P::dec4(L.cM, T.cM); P::dec4(L.cH, T.cH); P::dec4(L.cH2, T.cH2);
                 P::dec4(L.mxz, T.mxz);
                 P::dec4(L.op, T.op); P::dec4(L.oxx, T.oxx); P::dec4(L.ozz, T.ozz); P::dec4(L.oxz, T.oxz);
-                if constexpr (P::prec == BP_PREC_COMP16) {    // old state takes this step's rescale
+                if (P::prec == BP_PREC_COMP16 && r != (R)1) {    // old state takes this step's rescale
                     scale4(T.op, r); scale4(T.oxx, r); scale4(T.ozz, r); scale4(T.oxz, r);
                 }
             }
@@ -329,7 +332,10 @@ __global__ void __launch_bounds__(kMarchThreads, BP_MARCH_MINB) k_march(const Sh
                 T.wz[j] = dz_bwd<ORD, P>(wwz, j, S);                    // vwz: D-z
                 T.uxz[j] = dz_fwd<ORD, P>(wux, j, S);                   // vux: D+z
             }
-            if (act) t_tail<2, ORD, P, !kLean>(S, c, x0, 0, z, r, mask, T);
+            if (act) {
+                if (P::prec == BP_PREC_COMP16 && r != (R)1) t_tail<2, ORD, P, !kLean, true>(S, c, x0, 0, z, r, mask, T);
+                else t_tail<2, ORD, P, !kLean, false>(S, c, x0, 0, z, r, mask, T);
+            }
             shift(wux);
             shift(wuz);
             shift(wwz);
