@@ -83,3 +83,26 @@ def test_server_rejects_oversized_request():
         srv.submit(c, m)
     assert e.value.code == BP_ERR_BUDGET
     srv.close()
+
+
+def test_sharded_server_on_the_visible_devices():
+    """The shot-sharded router over every visible GPU (one here): results are
+    bit-identical to single runs, and the per-device totals add up."""
+    import torch
+    from mixedprecisionfaracoustic_b200.sharded import ShardedServer
+    reqs = config4_requests(seed=6, n=5, precision="comp16", scale=0.05, steps=(60, 150), include_3d=True)
+    singles = [alone(c, m)[0] for c, m in reqs]
+    devs = list(range(torch.cuda.device_count()))
+    srv = ShardedServer(devs, hbm_budget_bytes=8 << 30, steps_per_sync=20)
+    ids = [srv.submit(c, m) for c, m in reqs]
+    for gid in ids:
+        srv.wait(gid, 300)
+    for gid, ref in zip(ids, singles):
+        assert srv.poll(gid) == "done"
+        assert np.array_equal(srv.traces(gid, "txx"), ref)
+        assert srv.device_of(gid) in devs
+    assert srv.stats()["completed"] == len(reqs)
+    for gid in ids:
+        srv.release(gid)
+    assert all(v == 0 for v in srv.outstanding.values())
+    srv.close()
