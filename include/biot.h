@@ -141,6 +141,10 @@ int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out);
  * five traces (:1085-1093) -> snapshot if `it` is listed (:1094-1163).
  * Asynchronous on the simulation's stream; bp_sync waits. */
 int bp_run(bp_sim* sim, int nsteps);
+/* Waits for the issued steps.  BP_ERR_UNSTABLE if a recorded receiver value
+ * has gone non-finite (the run blew up: dt above the stability limit with
+ * check_cfl off, or a broken medium); bp_last_error names the first such step.
+ * The same check ends a served request as failed at the next sync point. */
 int bp_sync(bp_sim* sim);
 /* bp_run bracketed by CUDA events recorded on the simulation's stream; waits
  * and returns the device time of the nsteps steps in *ms. */

@@ -233,6 +233,14 @@ int bp_batch_sync(bp_batch* b) {
     if (!b) { set_error("null batch"); return BP_ERR_ARG; }
     cudaError_t e = cudaStreamSynchronize(b->st);
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
+    for (size_t i = 0; i < b->core.shots.size(); i++) {
+        const int bad = b->core.shots[i]->blowup_step(b->st);
+        if (bad) {
+            set_error("shot " + std::to_string(i) + ": non-finite value recorded at a receiver at step " +
+                      std::to_string(bad - 1));
+            return BP_ERR_UNSTABLE;
+        }
+    }
     return BP_OK;
 }
 

@@ -89,6 +89,7 @@ struct ShotDesc {
     int src_rec;                  // receiver index that owns the source cell, or -1
     long long tile0s;             // first tile of this shot in the TMA-staged 2D tiling
     int nseg_s;                   // 256-cell segments per row in that tiling
+    int* blowup;                  // first step (+1) with a non-finite recorded value, 0 = none
     int ncol_m;                   // marching 2D kernels: 128-cell columns per row
     long long tile0m;             // first task of this shot in the marching tiling
     int zseg_m;                   // rows per marching task

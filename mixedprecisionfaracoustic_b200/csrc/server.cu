@@ -171,13 +171,16 @@ static void server_loop(bp_server* s) {
                     std::lock_guard<std::mutex> g(s->mu);
                     cancel = r->cancel;
                 }
-                if (sh->it_host < sh->cfg.nt && !cancel) {
+                // a shot whose recorded values went non-finite is retired at
+                // once as failed instead of running to its last step
+                const int bad = sh->blowup_step(cb.st);
+                if (sh->it_host < sh->cfg.nt && !cancel && !bad) {
                     keep.push_back(r);
                     keep_shots.push_back(std::move(cb.core.shots[i]));
                     continue;
                 }
                 std::vector<float> tr;
-                if (!cancel) {
+                if (!cancel && !bad) {
                     const size_t nt = sh->cfg.nt, nr = sh->cfg.nrec;
                     std::vector<float> u((size_t)BP_NTRACE * sh->nurec * nt);
                     if (!u.empty()) cudaMemcpy(u.data(), sh->desc.traces, u.size() * 4, cudaMemcpyDeviceToHost);
@@ -193,9 +196,12 @@ static void server_loop(bp_server* s) {
                 r->shot = nullptr;
                 r->traces.swap(tr);
                 r->t_done = Clock::now();
-                r->state = cancel ? BP_REQ_CANCELLED : BP_REQ_DONE;
+                r->state = cancel ? BP_REQ_CANCELLED : (bad ? BP_REQ_FAILED : BP_REQ_DONE);
                 if (cancel) s->cancelled++;
-                else {
+                else if (bad) {
+                    r->err = "non-finite value recorded at a receiver at step " + std::to_string(bad - 1);
+                    s->failed++;
+                } else {
                     s->completed++;
                     s->latencies.push_back(std::chrono::duration<double>(r->t_done - r->t_submit).count());
                 }

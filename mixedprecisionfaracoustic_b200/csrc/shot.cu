@@ -95,7 +95,7 @@ struct Plan {
     // offsets
     size_t o_f[BP_NFIELDS], o_flo[BP_NFIELDS], o_vc[VC_COUNT], o_vclo[VC_COUNT], o_tc[TC_COUNT], o_tclo[TC_COUNT];
     size_t o_prof[3][4], o_psiV[3], o_psiT[3];
-    size_t o_tr, o_tr64, o_wav, o_dyn, o_rtab, o_rec, o_step, o_snap, o_scratch, o_out, o_desc;
+    size_t o_tr, o_tr64, o_wav, o_dyn, o_rtab, o_rec, o_step, o_blowup, o_snap, o_scratch, o_out, o_desc;
     size_t total;
     size_t staging;               // transient medium upload
 };
@@ -186,6 +186,7 @@ void make_plan(const bp_config* c, int nurec, Plan& p) {
     p.o_rtab = A.take((size_t)c->nt * 4);
     p.o_rec = A.take((size_t)nurec * 8 + 8);
     p.o_step = A.take(4);
+    p.o_blowup = A.take(4);
     p.o_snap = A.take((size_t)p.ncapt * p.snap_n * 4 + 4);
     const int nb = scan_kr_blocks() > reduce_blocks() ? scan_kr_blocks() : reduce_blocks();
     p.o_scratch = A.take((size_t)2 * nb * 8);
@@ -301,6 +302,7 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     S.rec_idx = (const long long*)at(p.o_rec);
     S.nrec = nurec;
     S.step_base = (int*)at(p.o_step);
+    S.blowup = (int*)at(p.o_blowup);
     S.src_mask = c->src_mask;
     S.src_idx_valid = c->src_mask != 0;
     S.src_idx = c->src_x + (long long)(dim == 3 ? c->src_y : 0) * pitch + (long long)c->src_z * pitch * nyp;
@@ -556,6 +558,15 @@ void arena_release(void* ptr, size_t bytes) {
 void release_cached_arenas(int device) {
     std::lock_guard<std::mutex> g(g_arena_mu);
     free_cached(device);
+}
+
+int Shot::blowup_step(cudaStream_t st) const {
+    int h = 0;
+    if (!desc.blowup) return 0;
+    if (cudaMemcpyAsync(&h, desc.blowup, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return 0;
+    return h;
 }
 
 void Shot::destroy() {

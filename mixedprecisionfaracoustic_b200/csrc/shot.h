@@ -91,6 +91,9 @@ struct Shot {
     // phases, recorded traces, captured snapshots.  Everything else in the
     // arena is fixed by the configuration and medium.
     std::vector<std::pair<void*, size_t>> state_regions() const;
+    // 1 + the first step whose recorded receiver values were not all finite,
+    // 0 if none (synchronises st).
+    int blowup_step(cudaStream_t st) const;
 
     // Computes the arena size for cfg without allocating (admission control).
     static int plan_bytes(const bp_config* cfg, size_t* bytes);

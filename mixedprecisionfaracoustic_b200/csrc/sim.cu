@@ -172,6 +172,12 @@ int bp_sync(bp_sim* s) {
     SIM_CK(cudaStreamSynchronize(s->st));
     int rc = s->run.device_error();
     if (rc) { set_error("a staged phase kernel gave up waiting for its tile copies"); return rc; }
+    const int bad = s->shot.blowup_step(s->st);
+    if (bad) {
+        set_error("non-finite value recorded at a receiver at step " + std::to_string(bad - 1) +
+                  " (dt above the stability limit?)");
+        return BP_ERR_UNSTABLE;
+    }
     return BP_OK;
 }
 

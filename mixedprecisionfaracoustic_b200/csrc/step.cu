@@ -373,11 +373,16 @@ __global__ void k_post(const ShotDesc* __restrict__ shots, int k, int do_record)
         v[BP_TR_VWX] = read_phys<P>(S, BP_F_VWX, i, sv);
         v[BP_TR_P] = read_phys<P>(S, BP_F_P, i, ss);
         const long long cs = (long long)S.nrec * S.nt;
+        bool finite = true;
 #pragma unroll
         for (int q = 0; q < BP_NTRACE; q++) {
             S.traces[q * cs + (long long)r * S.nt + it] = (float)v[q];
             if constexpr (P::prec == BP_PREC_FP64) S.traces64[q * cs + (long long)r * S.nt + it] = v[q];
+            finite = finite && isfinite(v[q]);
         }
+        // blow-up detection: the first step whose recorded values are not all
+        // finite (step + 1; 0 = none), read by the host at its next sync
+        if (!finite) atomicCAS(S.blowup, 0, it + 1);
     }
     const bool owner = (S.src_rec >= 0) ? (r == S.src_rec) : (blockIdx.x == 0 && threadIdx.x == 0);
     if (owner) inject<P>(S, it + 1);
