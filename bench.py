@@ -52,10 +52,11 @@ def parse():
     ap.add_argument("--nz", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=20)
-    ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4"], default="c1",
-                    help="c1: one 2D shot (default, the headline); c2: one 3D 512x512x384 shot; "
-                         "c3: 64 batched 2D shots; c4: serving stream")
+    ap.add_argument("--workload", choices=["c0", "c1", "c2", "c3", "c4"], default="c1",
+                    help="c1: one 2D shot (default, the headline); c0: the 3D 160^3 order-4 homogeneous shot; "
+                         "c2: one 3D 512x512x384 shot; c3: 64 batched 2D shots; c4: serving stream")
     ap.add_argument("--crop-steps", type=int, default=1000, help="c2: steps of the 128^3 crop accuracy runs")
+    ap.add_argument("--c0-steps", type=int, default=1000, help="c0: steps of each run (1000 in the configuration)")
     ap.add_argument("--scale", type=float, default=1.0, help="c3/c4: linear size scale of every shot")
     ap.add_argument("--requests", type=int, default=200, help="c4: number of requests")
     ap.add_argument("--precision", choices=["fp32", "comp16"], default="fp32", help="c3/c4 precision")
@@ -344,6 +345,50 @@ def run_batch(args, rank, ws):
             "clocks": clk.summary(), "timing": "host wall clock around bp_batch_run + bp_batch_sync"}
 
 
+def run_c0(args):
+    """c0: 3D homogeneous 160^3 (+20-cell CPML = 200^3), order 4, 1000 steps, FP32
+    and COMP16: Mcell-updates/s, phase HBM GB/s vs the measured peak, and the
+    seismogram rel-L2 of each against an FP64 run of the same 1000 steps."""
+    import torch
+    from mixedprecisionfaracoustic_b200 import Simulation
+    from mixedprecisionfaracoustic_b200.presets import config0
+    torch.cuda.set_device(0)
+    nt = max(args.c0_steps, 30)
+    peak, peak_kind = measured_peaks()
+    runs = {}
+    res = {}
+    for prec in ("fp64", "fp32", "comp16"):
+        cfg, med = config0(precision=prec, order=4, nt=nt)
+        s = Simulation(cfg, med)
+        s.run(5)
+        s.sync()
+        with ClockSampler(0) as clk:
+            ms = s.run_timed(nt - 5 - 10)
+        (bv, bt), cells = s.algorithmic_bytes()
+        pv, pt, pp = s.profile_phases(10)
+        s.sync()
+        runs[prec] = s
+        res[prec] = {"value": cells * (nt - 15) / (ms * 1e-3) / 1e6, "ms_per_step": ms / (nt - 15),
+                     "phase_ms": {"v_phase": pv, "t_phase": pt, "record_inject": pp},
+                     "frac": {"v_phase": bv * cells / (pv * 1e-3) / 1e9 / peak,
+                              "t_phase": bt * cells / (pt * 1e-3) / 1e9 / peak,
+                              "step": (bv + bt) * cells / ((pv + pt) * 1e-3) / 1e9 / peak},
+                     "cells": cells, "clocks": clk.summary()}
+    for prec in ("fp32", "comp16"):
+        res[prec]["rel_l2_vs_fp64"] = {c: runs[prec].trace_rel_l2(runs["fp64"], c) for c in ("txx", "tzz", "vux", "p")}
+    for s in runs.values():
+        s.close()
+    f32 = res["fp32"]
+    return {"metric": METRIC, "value": f32["value"], "unit": METRIC, "n_gpus": 1, "steps": nt - 15, "warmup": 5,
+            "ms_per_step": f32["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"c0: 3D homogeneous 160^3 (+20-cell CPML = 200^3), order 4, 128 receivers, "
+                                   f"{nt} steps", "l2_flush": "inputs larger than L2 (1.9 GB working set)"},
+            "roofline": {"bound": "hbm", "kernel": "step", "achieved": f32["frac"]["step"] * peak, "peak": peak,
+                         "unit": "GB/s", "frac": f32["frac"]["step"], "peak_source": peak_kind},
+            "fp32": f32, "comp16": res["comp16"], "fp64": {k: res["fp64"][k] for k in ("value", "ms_per_step")}}
+
+
 def run_c2(args):
     """c2: the 3D 512x512x384 log-normal model (+20-cell CPML), COMP16 and FP32:
     Mcell-updates/s and the phase kernels' HBM GB/s against the measured peak;
@@ -452,9 +497,9 @@ def run_serve(args, rank):
 def main():
     args = parse()
     ws, rank, local = dist_env()
-    if args.workload == "c2" and args.impl == "ours":
+    if args.workload in ("c0", "c2") and args.impl == "ours":
         if rank == 0:
-            print(json.dumps(run_c2(args)), flush=True)
+            print(json.dumps(run_c0(args) if args.workload == "c0" else run_c2(args)), flush=True)
         return 0
     if args.workload != "c1" and args.impl == "ours":
         if ws > 1:

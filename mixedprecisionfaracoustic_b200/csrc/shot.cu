@@ -417,7 +417,7 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
 
     long long cx = p.nx - 2 * S.hw, cz = p.nz - 2 * S.hw, cy = dim == 3 ? p.ny - 2 * S.hw : 1;
     cells = cx * cy * cz;
-    ntiles = (long long)S.nseg * ((S.nrows + tile_rows() - 1) / tile_rows());
+    ntiles = (long long)S.nseg * tile_row_blocks(dim, c->precision, S.ny, S.nz);
     ntiles_s = (long long)S.nseg_s * ((S.nrows + staged_tile_rows() - 1) / staged_tile_rows());
     ntiles_m = dim == 2 ? (long long)S.ncol_m * ((p.nz - 2 * S.hw + S.zseg_m - 1) / S.zseg_m) : 0;
     it_host = 0;

@@ -24,6 +24,7 @@ cudaError_t launch_field_f64(int prec, const ShotDesc* d_shots, int f, double* o
 cudaError_t launch_coef(int prec, const ShotDesc* d_shots, int which, float* out, cudaStream_t st);
 int phase_threads();
 int tile_rows();
+long long tile_row_blocks(int dim, int prec, int ny, int nz);   // row blocks of the tile kernels per shot
 int seg_cells();
 // TMA-staged 2D phase kernels (step_staged.cu)
 bool staged_supported(int prec, int dim);
