@@ -69,8 +69,10 @@ __device__ __forceinline__ int locate_shot(const ShotDesc* shots, int nshots, lo
 #ifndef BP_MINB3_C16
 #define BP_MINB3_C16 4
 #endif
-template <int DIM, class P, bool VPHASE>
+template <int DIM, int ORD, class P, bool VPHASE>
 __host__ __device__ constexpr int phase_min_blocks() {
+    // 3D COMP16 T at order 4 spills heavily at 64 registers: 3 CTAs (80) there
+    if (DIM == 3 && P::prec == BP_PREC_COMP16 && !VPHASE && ORD == 4) return 3;
     if (DIM == 3) return P::prec == BP_PREC_FP32 ? BP_MINB3_F32 : P::prec == BP_PREC_COMP16 ? BP_MINB3_C16 : 1;
     return P::prec == BP_PREC_FP32 ? BP_MINB_F32
                                    : P::prec == BP_PREC_COMP16 ? (VPHASE ? BP_MINB_C16_V : BP_MINB_C16) : 1;
@@ -258,7 +260,7 @@ __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z,
 // ---------------------------------------------------------------------------
 // Tile loop shared by both phases.
 template <int DIM, int ORD, class P, bool VPHASE>
-__global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, P, VPHASE>())) k_phase(const ShotDesc* __restrict__ shots, int nshots,
+__global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHASE>())) k_phase(const ShotDesc* __restrict__ shots, int nshots,
                                                      long long ntiles, int k) {
     using R = typename P::real;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
