@@ -300,6 +300,27 @@ def run_reference(args, rank, ws):
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def fp64_rel_l2(cfg, med, got, steps, min_signal=0.0):
+    """Seismogram rel-L2 of traces `got` (component -> [nrec, >= steps]) against an FP64
+    run of the same shot for `steps` steps; None if the FP64 traces never exceed
+    `min_signal` (the wave has not reached the receivers yet)."""
+    import copy
+    from mixedprecisionfaracoustic_b200 import Simulation
+    c = copy.copy(cfg)
+    c.precision = "fp64"
+    c.nt = steps
+    with Simulation(c, med) as s:
+        s.run(steps)
+        out = {}
+        for comp, a in got.items():
+            ref = s.traces(comp).astype(np.float64)
+            if np.abs(ref).max() <= min_signal:
+                return None
+            d = np.asarray(a, dtype=np.float64)[:, :steps]
+            out[comp] = float(np.linalg.norm(d - ref) / max(np.linalg.norm(ref), 1e-300))
+    return out
+
+
 def run_batch(args, rank, ws):
     """c3: 64 2D shots (sizes from {1024^2, 1536x1024, 2048^2, 3072x1536}) in one
     persistent launch per phase and graph-replayed chunks; this rank's share of
@@ -330,6 +351,17 @@ def run_batch(args, rank, ws):
         b.sync()
     el = max_over_ranks(time.perf_counter() - t0)
     upd = b.cell_updates() - u0
+    # accuracy against FP64 runs of the same steps, for the first three of this
+    # rank's shots whose receivers the wave has reached within those steps
+    acc = {}
+    for j in range(min(12, len(mine))):
+        if len(acc) == 3:
+            break
+        i = mine[j]
+        got = {c: b.traces(j, c) for c in ("txx", "p")}
+        r = fp64_rel_l2(shots[i][0], shots[i][1], got, W + K, min_signal=1e-6)
+        if r is not None:
+            acc[f"shot{i}"] = r
     tot = upd
     if ws > 1:
         t = torch.tensor([float(upd)], device="cuda", dtype=torch.float64)
@@ -342,7 +374,8 @@ def run_batch(args, rank, ws):
             "dtype": "f32" if args.precision == "fp32" else "f16+i8 storage, f32 math", "data": "synthetic",
             "config": {"workload": f"c3: 64 batched 2D shots x{args.scale} size, {args.precision}",
                        "shots_on_rank0": len(mine), "tune": tune, "parallelism": f"shots sharded over {ws}"},
-            "clocks": clk.summary(), "timing": "host wall clock around bp_batch_run + bp_batch_sync"}
+            "clocks": clk.summary(), "timing": "host wall clock around bp_batch_run + bp_batch_sync",
+            "rel_l2_vs_fp64_sample": acc}
 
 
 def run_c0(args):
@@ -482,6 +515,13 @@ def run_serve(args, rank):
         srv.wait(r, 3600)
     el = time.perf_counter() - t0
     lat = sorted(srv.latency(r) for r in ids)
+    # accuracy of a fixed sample of the requests (2D and 3D) against FP64 runs
+    acc = {}
+    sample = [i for i, (c, _) in enumerate(reqs) if c.dim == 2][:2] + [i for i, (c, _) in enumerate(reqs) if c.dim == 3][:1]
+    for i in sample:
+        c, m = reqs[i]
+        got = {comp: srv.traces(ids[i], comp) for comp in ("txx", "p")}
+        acc[f"req{i}_{c.dim}d"] = fp64_rel_l2(c, m, got, c.nt)
     st = srv.stats()
     srv.close()
     return {"metric": METRIC, "value": work / el / 1e6, "unit": METRIC, "n_gpus": 1, "steps": None, "warmup": 8,
@@ -491,7 +531,8 @@ def run_serve(args, rank):
                        "rate_per_s": rate, "capacity_cell_updates_per_s": cap, "hbm_budget_GB": 150},
             "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
             "server": {k: st[k] for k in ("completed", "max_resident", "busy_seconds", "cell_updates")},
-            "timing": "host wall clock from first submit to last completion"}
+            "timing": "host wall clock from first submit to last completion",
+            "rel_l2_vs_fp64_sample": acc}
 
 
 def main():
