@@ -60,20 +60,23 @@ __device__ __forceinline__ int locate_shot(const ShotDesc* shots, int nshots, lo
 #define BP_MINB_C16_V 6
 #endif
 // 3D: uncapped, the kernels take 128-169 registers (1-2 CTAs per SM); capped
-// at 3 CTAs (80 registers, ~150 bytes spilled) the 192^3 order-2 and 200^3
-// order-4 steps run 1.75-2.1x faster on B200, FP32 and COMP16 alike.  COMP16
-// gains another 7 % at 4 CTAs on the 552 x 552 x 424 order-2 grid.
+// at 3 CTAs (80 registers, ~130 bytes spilled) the 192^3 order-2 and 200^3
+// order-4 FP32 steps run 1.75-2.1x faster on B200.  COMP16, taken one output
+// group at a time (v_chunk3/t_chunk3, next to no spills), is fastest at 4 CTAs
+// (64 registers) on the 552 x 552 x 424 and 200^3 grids; FP64 at 2 (128
+// registers; uncapped it takes 196-240, one CTA per SM).
 #ifndef BP_MINB3_F32
 #define BP_MINB3_F32 3
 #endif
 #ifndef BP_MINB3_C16
 #define BP_MINB3_C16 4
 #endif
+#ifndef BP_MINB3_F64
+#define BP_MINB3_F64 2
+#endif
 template <int DIM, int ORD, class P, bool VPHASE>
 __host__ __device__ constexpr int phase_min_blocks() {
-    // 3D COMP16 T at order 4 spills heavily at 64 registers: 3 CTAs (80) there
-    if (DIM == 3 && P::prec == BP_PREC_COMP16 && !VPHASE && ORD == 4) return 3;
-    if (DIM == 3) return P::prec == BP_PREC_FP32 ? BP_MINB3_F32 : P::prec == BP_PREC_COMP16 ? BP_MINB3_C16 : 1;
+    if (DIM == 3) return P::prec == BP_PREC_FP32 ? BP_MINB3_F32 : P::prec == BP_PREC_COMP16 ? BP_MINB3_C16 : BP_MINB3_F64;
     return P::prec == BP_PREC_FP32 ? BP_MINB_F32
                                    : P::prec == BP_PREC_COMP16 ? (VPHASE ? BP_MINB_C16_V : BP_MINB_C16) : 1;
 }
@@ -258,6 +261,312 @@ __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z,
 }
 
 // ---------------------------------------------------------------------------
+// 3D chunks taken one output group at a time.  v_chunk/t_chunk form all twelve
+// derivatives of a 3D chunk before the CPML and the updates, so 48 values (96
+// in FP64) are live at once and the 80-register kernels spill.  Here each
+// velocity component (and each shear stress, then the normal stresses and
+// the pressure) loads, differences, CPML-corrects and stores only what it
+// needs.  Every element goes through the same operations in the same order
+// as in v_tail/t_tail, so the results are bit-identical.
+// Which phases take this form, per precision (bit 0 = V, bit 1 = T).
+// Measured on B200 (192^3 and 552 x 552 x 424 order 2, 200^3 order 4):
+// COMP16 both (12-16 % off the step, its spills gone); FP64 the T phase (with
+// 2 CTAs per SM, 25-30 % off the step); FP32 neither (up to 10 % slower, its
+// latency-bound phases losing the loads they had in flight).
+#ifndef BP_SPLIT3_C16
+#define BP_SPLIT3_C16 3
+#endif
+#ifndef BP_SPLIT3_F32
+#define BP_SPLIT3_F32 0
+#endif
+#ifndef BP_SPLIT3_F64
+#define BP_SPLIT3_F64 2
+#endif
+template <class P, bool VPHASE>
+__host__ __device__ constexpr bool split3() {
+    return ((P::prec == BP_PREC_COMP16 ? BP_SPLIT3_C16 : P::prec == BP_PREC_FP32 ? BP_SPLIT3_F32 : BP_SPLIT3_F64) >>
+            (VPHASE ? 0 : 1)) & 1;
+}
+
+// Difference along x of one field at the chunk (span load), divided by H.
+template <int ORD, class P, bool FWD>
+__device__ __forceinline__ void d_span(const ShotDesc& S, int f, long long row, int x0,
+                                       typename P::real (&d)[4]) {
+    typename P::real v[4 + ORD];
+    load_span<ORD, P>(S.f[f], S.flo[f], row, x0, S.nx, v);
+#pragma unroll
+    for (int j = 0; j < 4; j++) d[j] = deriv_div<P>(FWD ? dfwd<ORD>(v, j) : dbwd<ORD>(v, j), S);
+}
+// Difference across rows (y or z) of one field at the chunk, divided by H.
+template <int ORD, class P, bool FWD>
+__device__ __forceinline__ void d_rows(const ShotDesc& S, int f, long long c, long long stride,
+                                       typename P::real (&d)[4]) {
+    using R = typename P::real;
+    R a[ORD + 1][4];
+    load_rows<ORD, P>(S.f[f], S.flo[f], c, stride, a);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        R t[ORD + 1];
+#pragma unroll
+        for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
+        d[j] = deriv_div<P>(FWD ? rfwd<ORD>(t) : rbwd<ORD>(t), S);
+    }
+}
+// Masked cells feed zero derivatives into the memory variables.
+template <class R>
+__device__ __forceinline__ void mask0(R (&d)[4], unsigned mask) {
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        if (!(mask >> j & 1u)) d[j] = 0;
+}
+// CPML of one derivative on the slab of `axis` (slot k, half-grid profile if
+// half); nothing outside that slab.
+template <bool RS, class R>
+__device__ __forceinline__ void cpml3(const ShotDesc& S, void* const (&psi)[3], int axis, int k, bool half,
+                                      long long si, int x0, int y, int z, R (&d)[4], R r) {
+    if (si < 0) return;
+    const void* pb = half ? S.pb2[axis] : S.pb[axis];
+    const void* pe = half ? S.pe2[axis] : S.pe[axis];
+    cpml_slot<4, RS, R>(d, psi[axis], S.slab_cells[axis], k, si, axis == 0, axis == 0 ? x0 : (axis == 1 ? y : z),
+                        x0, pb, pe, r);
+}
+
+// One velocity component AX (0 = x, 1 = y, 2 = z) of the 3D V phase
+// (Float/main.cu:103-191 for that component).
+template <int ORD, class P, bool RS, int AX>
+__device__ __forceinline__ void v_comp3(const ShotDesc& S, long long c, long long row, int x0, int y, int z,
+                                        typename P::real r, unsigned mask, const typename P::real (&rf)[4]) {
+    using R = typename P::real;
+    const long long sy = S.pitch, sz = S.plane;
+    // dx, dy, dz: the stress derivatives summed into this component; dp: the
+    // pressure derivative along AX.  Slots as in v_tail.
+    R dx[4], dy[4], dz[4], dp[4];
+    if constexpr (AX == 0) {
+        d_span<ORD, P, true>(S, BP_F_TXX, row, x0, dx);     // x1
+        d_rows<ORD, P, false>(S, BP_F_TXY, c, sy, dy);      // x2
+        d_rows<ORD, P, false>(S, BP_F_TXZ, c, sz, dz);      // x3
+        d_span<ORD, P, true>(S, BP_F_P, row, x0, dp);       // s1
+    } else if constexpr (AX == 1) {
+        d_span<ORD, P, false>(S, BP_F_TXY, row, x0, dx);    // y2
+        d_rows<ORD, P, true>(S, BP_F_TYY, c, sy, dy);       // y1
+        d_rows<ORD, P, false>(S, BP_F_TYZ, c, sz, dz);      // y3
+        d_rows<ORD, P, true>(S, BP_F_P, c, sy, dp);         // s2
+    } else {
+        d_span<ORD, P, false>(S, BP_F_TXZ, row, x0, dx);    // z2
+        d_rows<ORD, P, false>(S, BP_F_TYZ, c, sy, dy);      // z3
+        d_rows<ORD, P, true>(S, BP_F_TZZ, c, sz, dz);       // z1
+        d_rows<ORD, P, true>(S, BP_F_P, c, sz, dp);         // s3
+    }
+    if constexpr (P::prec == BP_PREC_COMP16 && RS) { scale4(dx, r); scale4(dy, r); scale4(dz, r); scale4(dp, r); }
+    mask0(dx, mask); mask0(dy, mask); mask0(dz, mask); mask0(dp, mask);
+    void* const psi[3] = {S.psiV[0], S.psiV[1], S.psiV[2]};
+    const long long s0 = slab_index(S, 0, x0, y, z), s1 = slab_index(S, 1, x0, y, z),
+                    s2 = slab_index(S, 2, x0, y, z);
+    if constexpr (AX == 0) {
+        cpml3<RS>(S, psi, 0, 0, true, s0, x0, y, z, dx, r);
+        cpml3<RS>(S, psi, 0, 1, true, s0, x0, y, z, dp, r);
+        cpml3<RS>(S, psi, 1, 0, false, s1, x0, y, z, dy, r);
+        cpml3<RS>(S, psi, 2, 0, false, s2, x0, y, z, dz, r);
+    } else if constexpr (AX == 1) {
+        cpml3<RS>(S, psi, 0, 3, false, s0, x0, y, z, dx, r);
+        cpml3<RS>(S, psi, 1, 1, true, s1, x0, y, z, dy, r);
+        cpml3<RS>(S, psi, 1, 2, true, s1, x0, y, z, dp, r);
+        cpml3<RS>(S, psi, 2, 3, false, s2, x0, y, z, dz, r);
+    } else {
+        cpml3<RS>(S, psi, 0, 2, false, s0, x0, y, z, dx, r);
+        cpml3<RS>(S, psi, 1, 3, false, s1, x0, y, z, dy, r);
+        cpml3<RS>(S, psi, 2, 1, true, s2, x0, y, z, dz, r);
+        cpml3<RS>(S, psi, 2, 2, true, s2, x0, y, z, dp, r);
+    }
+    // the divergence in v_tail's summation order: x1+x2+x3, y1+y2+y3, z1+z2+z3
+    R sum[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if constexpr (AX == 0) sum[j] = dx[j] + dy[j] + dz[j];
+        else if constexpr (AX == 1) sum[j] = dy[j] + dx[j] + dz[j];
+        else sum[j] = dz[j] + dx[j] + dy[j];
+    }
+    constexpr int fu = AX == 0 ? BP_F_VUX : AX == 1 ? BP_F_VUY : BP_F_VUZ;
+    constexpr int fw = AX == 0 ? BP_F_VWX : AX == 1 ? BP_F_VWY : BP_F_VWZ;
+    constexpr int crho = AX == 0 ? VC_RHO_X : AX == 1 ? VC_RHO_Y : VC_RHO_Z;
+    constexpr int cc1 = AX == 0 ? VC_CC1_X : AX == 1 ? VC_CC1_Y : VC_CC1_Z;
+    constexpr int cc2 = AX == 0 ? VC_CC2_X : AX == 1 ? VC_CC2_Y : VC_CC2_Z;
+    R rho[4], c1[4], c2[4], vu[4], vw[4], nu[4], nw[4];
+    P::ld4(S.vc[crho], S.vclo[crho], c, rho);
+    P::ld4(S.vc[cc1], S.vclo[cc1], c, c1);
+    P::ld4(S.vc[cc2], S.vclo[cc2], c, c2);
+    P::ld4(S.f[fu], S.flo[fu], c, vu);
+    P::ld4(S.f[fw], S.flo[fw], c, vw);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if constexpr (P::prec == BP_PREC_COMP16) {
+            const R wo = RS ? mulr(vw[j], r) : vw[j], uo = RS ? mulr(vu[j], r) : vu[j];
+            R rr = rf[j] * rho[j];
+            R wn = c1[j] * wo - (rr * c2[j]) * sum[j] - c2[j] * dp[j];
+            nw[j] = wn;
+            nu[j] = uo + rho[j] * sum[j] - rr * (wn - wo);
+        } else {
+            R wo = vw[j];
+            const R num = wo * c2[j] - S.dtr<R>() * (rf[j] * rho[j] * sum[j] + dp[j]);
+            const R wn = (c1[j] == (R)0) ? (R)0 : (num == (R)0 ? num * c1[j] : num / c1[j]);
+            nw[j] = wn;
+            nu[j] = vu[j] + S.dtr<R>() * rho[j] * sum[j] - rf[j] * rho[j] * (wn - wo);
+        }
+        if (!(mask >> j & 1u)) { nw[j] = vw[j]; nu[j] = vu[j]; }
+    }
+    P::st4(S.f[fw], S.flo[fw], c, nw);
+    P::st4(S.f[fu], S.flo[fu], c, nu);
+}
+
+template <int ORD, class P, bool RS>
+__device__ __forceinline__ void v_chunk3(const ShotDesc& S, int x0, int y, int z, typename P::real r,
+                                         unsigned mask) {
+    using R = typename P::real;
+    const long long c = x0 + (long long)y * S.pitch + (long long)z * S.plane;
+    const long long row = c - x0;
+    R rf[4];
+    P::ld4(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, rf);
+    v_comp3<ORD, P, RS, 0>(S, c, row, x0, y, z, r, mask, rf);
+    v_comp3<ORD, P, RS, 1>(S, c, row, x0, y, z, r, mask, rf);
+    v_comp3<ORD, P, RS, 2>(S, c, row, x0, y, z, r, mask, rf);
+}
+
+// Old value of a stress field at the chunk, with this step's rescale.
+template <class P, bool RS>
+__device__ __forceinline__ void ld_old(const ShotDesc& S, int f, long long c, typename P::real r,
+                                       typename P::real (&o)[4]) {
+    P::ld4(S.f[f], S.flo[f], c, o);
+    if constexpr (P::prec == BP_PREC_COMP16 && RS) scale4(o, r);
+}
+template <class P>
+__device__ __forceinline__ void st_new(const ShotDesc& S, int f, long long c, unsigned mask,
+                                       typename P::real (&nv)[4], const typename P::real (&ov)[4]) {
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        if (!(mask >> j & 1u)) nv[j] = ov[j];
+    P::st4(S.f[f], S.flo[f], c, nv);
+}
+
+// One shear stress of the 3D T phase: SH 0 = txy, 1 = tyz, 2 = txz
+// (Float/main.cu:232-294 for that stress).
+template <int ORD, class P, bool RS, int SH>
+__device__ __forceinline__ void t_shear3(const ShotDesc& S, long long c, long long row, int x0, int y, int z,
+                                         typename P::real r, unsigned mask, void* const (&psi)[3]) {
+    using R = typename P::real;
+    const long long sy = S.pitch, sz = S.plane;
+    R a[4], b[4];    // the two derivatives, in the order of the update's sum
+    if constexpr (SH == 0) {
+        d_rows<ORD, P, true>(S, BP_F_VUX, c, sy, a);        // uxy
+        d_span<ORD, P, true>(S, BP_F_VUY, row, x0, b);      // uyx
+    } else if constexpr (SH == 1) {
+        d_rows<ORD, P, true>(S, BP_F_VUY, c, sz, a);        // uyz
+        d_rows<ORD, P, true>(S, BP_F_VUZ, c, sy, b);        // uzy
+    } else {
+        d_rows<ORD, P, true>(S, BP_F_VUX, c, sz, a);        // uxz
+        d_span<ORD, P, true>(S, BP_F_VUZ, row, x0, b);      // uzx
+    }
+    mask0(a, mask); mask0(b, mask);
+    if constexpr (SH == 0) {
+        cpml3<RS>(S, psi, 0, 3, true, slab_index(S, 0, x0, y, z), x0, y, z, b, r);
+        cpml3<RS>(S, psi, 1, 2, true, slab_index(S, 1, x0, y, z), x0, y, z, a, r);
+    } else if constexpr (SH == 1) {
+        cpml3<RS>(S, psi, 1, 3, true, slab_index(S, 1, x0, y, z), x0, y, z, b, r);
+        cpml3<RS>(S, psi, 2, 3, true, slab_index(S, 2, x0, y, z), x0, y, z, a, r);
+    } else {
+        cpml3<RS>(S, psi, 0, 2, true, slab_index(S, 0, x0, y, z), x0, y, z, b, r);
+        cpml3<RS>(S, psi, 2, 2, true, slab_index(S, 2, x0, y, z), x0, y, z, a, r);
+    }
+    constexpr int f = SH == 0 ? BP_F_TXY : SH == 1 ? BP_F_TYZ : BP_F_TXZ;
+    constexpr int cm = SH == 0 ? TC_MUXY : SH == 1 ? TC_MUYZ : TC_MUXZ;
+    R mu[4], o[4], n[4];
+    P::ld4(S.tc[cm], S.tclo[cm], c, mu);
+    ld_old<P, RS>(S, f, c, r, o);
+    const R dt = S.dtr<R>();
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if constexpr (P::prec == BP_PREC_COMP16) n[j] = o[j] + mu[j] * (a[j] + b[j]);
+        else n[j] = o[j] + mu[j] * dt * (a[j] + b[j]);
+    }
+    st_new<P>(S, f, c, mask, n, o);
+}
+
+template <int ORD, class P, bool RS>
+__device__ __forceinline__ void t_chunk3(const ShotDesc& S, int x0, int y, int z, typename P::real r,
+                                         unsigned mask) {
+    using R = typename P::real;
+    const long long sy = S.pitch, sz = S.plane;
+    const long long c = x0 + (long long)y * sy + (long long)z * sz;
+    const long long row = c - x0;
+    void* const psi[3] = {S.psiT[0], S.psiT[1], S.psiT[2]};
+    t_shear3<ORD, P, RS, 0>(S, c, row, x0, y, z, r, mask, psi);
+    t_shear3<ORD, P, RS, 1>(S, c, row, x0, y, z, r, mask, psi);
+    t_shear3<ORD, P, RS, 2>(S, c, row, x0, y, z, r, mask, psi);
+
+    // normal stresses and pressure: the six divergence derivatives
+    R uxx[4], uyy[4], uzz[4], wx[4], wy[4], wz[4];
+    d_span<ORD, P, false>(S, BP_F_VUX, row, x0, uxx);
+    d_span<ORD, P, false>(S, BP_F_VWX, row, x0, wx);
+    d_rows<ORD, P, false>(S, BP_F_VUY, c, sy, uyy);
+    d_rows<ORD, P, false>(S, BP_F_VWY, c, sy, wy);
+    d_rows<ORD, P, false>(S, BP_F_VUZ, c, sz, uzz);
+    d_rows<ORD, P, false>(S, BP_F_VWZ, c, sz, wz);
+    mask0(uxx, mask); mask0(wx, mask); mask0(uyy, mask); mask0(wy, mask); mask0(uzz, mask); mask0(wz, mask);
+    {
+        const long long s0 = slab_index(S, 0, x0, y, z);
+        cpml3<RS>(S, psi, 0, 0, false, s0, x0, y, z, uxx, r);
+        cpml3<RS>(S, psi, 0, 1, false, s0, x0, y, z, wx, r);
+        const long long s1 = slab_index(S, 1, x0, y, z);
+        cpml3<RS>(S, psi, 1, 0, false, s1, x0, y, z, uyy, r);
+        cpml3<RS>(S, psi, 1, 1, false, s1, x0, y, z, wy, r);
+        const long long s2 = slab_index(S, 2, x0, y, z);
+        cpml3<RS>(S, psi, 2, 0, false, s2, x0, y, z, uzz, r);
+        cpml3<RS>(S, psi, 2, 1, false, s2, x0, y, z, wz, r);
+    }
+    R cC[4], cM[4], cH[4], cH2[4], o[4], n[4];
+    const R dt = S.dtr<R>();
+    P::ld4(S.tc[TC_C], S.tclo[TC_C], c, cC);
+    P::ld4(S.tc[TC_M], S.tclo[TC_M], c, cM);
+    ld_old<P, RS>(S, BP_F_P, c, r, o);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if constexpr (P::prec == BP_PREC_COMP16)
+            n[j] = o[j] - cC[j] * (uxx[j] + uyy[j] + uzz[j]) - cM[j] * (wx[j] + wy[j] + wz[j]);
+        else
+            n[j] = o[j] - dt * (cC[j] * (uxx[j] + uyy[j] + uzz[j]) + cM[j] * (wx[j] + wy[j] + wz[j]));
+    }
+    st_new<P>(S, BP_F_P, c, mask, n, o);
+    P::ld4(S.tc[TC_H], S.tclo[TC_H], c, cH);
+    P::ld4(S.tc[TC_H2U], S.tclo[TC_H2U], c, cH2);
+    ld_old<P, RS>(S, BP_F_TXX, c, r, o);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if constexpr (P::prec == BP_PREC_COMP16)
+            n[j] = o[j] + cH2[j] * (uyy[j] + uzz[j]) + cH[j] * uxx[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
+        else
+            n[j] = o[j] + dt * (cH2[j] * (uyy[j] + uzz[j]) + cH[j] * uxx[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
+    }
+    st_new<P>(S, BP_F_TXX, c, mask, n, o);
+    ld_old<P, RS>(S, BP_F_TYY, c, r, o);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if constexpr (P::prec == BP_PREC_COMP16)
+            n[j] = o[j] + cH2[j] * (uxx[j] + uzz[j]) + cH[j] * uyy[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
+        else
+            n[j] = o[j] + dt * (cH2[j] * (uxx[j] + uzz[j]) + cH[j] * uyy[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
+    }
+    st_new<P>(S, BP_F_TYY, c, mask, n, o);
+    ld_old<P, RS>(S, BP_F_TZZ, c, r, o);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if constexpr (P::prec == BP_PREC_COMP16)
+            n[j] = o[j] + cH2[j] * (uxx[j] + uyy[j]) + cH[j] * uzz[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
+        else
+            n[j] = o[j] + dt * (cH2[j] * (uxx[j] + uyy[j]) + cH[j] * uzz[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
+    }
+    st_new<P>(S, BP_F_TZZ, c, mask, n, o);
+}
+
+// ---------------------------------------------------------------------------
 // Tile loop shared by both phases.
 template <int DIM, int ORD, class P, bool VPHASE>
 __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHASE>())) k_phase(const ShotDesc* __restrict__ shots, int nshots,
@@ -329,7 +638,15 @@ __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHAS
         // COMP16: the rescale products only on the steps whose factor is not
         // exactly 1 (a uniform branch; the products are never fused, so both
         // forms give the same bits when r == 1)
-        if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
+        if constexpr (DIM == 3 && split3<P, VPHASE>()) {
+            if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
+                if constexpr (VPHASE) v_chunk3<ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+                else t_chunk3<ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+            } else {
+                if constexpr (VPHASE) v_chunk3<ORD, P, false>(S, x0, y, z, r, mask);
+                else t_chunk3<ORD, P, false>(S, x0, y, z, r, mask);
+            }
+        } else if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
             if constexpr (VPHASE) v_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
             else t_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
         } else {
