@@ -45,24 +45,28 @@ __device__ __forceinline__ int locate_shot(const ShotDesc* shots, int nshots, lo
 #ifndef BP_RS_SPLIT
 #define BP_RS_SPLIT 1
 #endif
-// Resident CTAs per SM the 2D FP32/COMP16 phase kernels are register-limited
-// to (1 = no limit).  Measured on B200 for the 4040 x 2040 order-2 grid: FP32
-// is fastest at 3 (80 registers, no spills); COMP16, whose decode/encode
-// chains leave it latency-bound, at 6 for the V phase (40 registers) and 5 for
-// the T phase (48 registers), both with some spilled values.
+// Resident CTAs per SM the 2D phase kernels are register-limited to (1 = no
+// limit).  Measured on B200 for the 4040 x 2040 order-2 grid: FP32 is fastest
+// at 3 (80 registers, no spills); COMP16, whose decode/encode chains leave it
+// latency-bound, at 6 (40 registers) for both phases, the T phase in grouped
+// form (below), both with some spilled values; FP64 at 2 (128 registers;
+// uncapped it takes ~150, one CTA per SM, and runs 40 % slower).
 #ifndef BP_MINB_F32
 #define BP_MINB_F32 3
 #endif
 #ifndef BP_MINB_C16
-#define BP_MINB_C16 5
+#define BP_MINB_C16 6
 #endif
 #ifndef BP_MINB_C16_V
 #define BP_MINB_C16_V 6
 #endif
+#ifndef BP_MINB_F64
+#define BP_MINB_F64 2
+#endif
 // 3D: uncapped, the kernels take 128-169 registers (1-2 CTAs per SM); capped
 // at 3 CTAs (80 registers, ~130 bytes spilled) the 192^3 order-2 and 200^3
 // order-4 FP32 steps run 1.75-2.1x faster on B200.  COMP16, taken one output
-// group at a time (v_chunk3/t_chunk3, next to no spills), is fastest at 4 CTAs
+// group at a time (v_chunk_g/t_chunk_g, next to no spills), is fastest at 4 CTAs
 // (64 registers) on the 552 x 552 x 424 and 200^3 grids; FP64 at 2 (128
 // registers; uncapped it takes 196-240, one CTA per SM).
 #ifndef BP_MINB3_F32
@@ -78,7 +82,7 @@ template <int DIM, int ORD, class P, bool VPHASE>
 __host__ __device__ constexpr int phase_min_blocks() {
     if (DIM == 3) return P::prec == BP_PREC_FP32 ? BP_MINB3_F32 : P::prec == BP_PREC_COMP16 ? BP_MINB3_C16 : BP_MINB3_F64;
     return P::prec == BP_PREC_FP32 ? BP_MINB_F32
-                                   : P::prec == BP_PREC_COMP16 ? (VPHASE ? BP_MINB_C16_V : BP_MINB_C16) : 1;
+                                   : P::prec == BP_PREC_COMP16 ? (VPHASE ? BP_MINB_C16_V : BP_MINB_C16) : BP_MINB_F64;
 }
 // How a tile learns its step index: 1 = once per shot per launch, 0 = a read
 // of the step counter per tile (measured faster for FP32 at 80 registers).
@@ -261,31 +265,43 @@ __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z,
 }
 
 // ---------------------------------------------------------------------------
-// 3D chunks taken one output group at a time.  v_chunk/t_chunk form all twelve
-// derivatives of a 3D chunk before the CPML and the updates, so 48 values (96
-// in FP64) are live at once and the 80-register kernels spill.  Here each
+// Chunks taken one output group at a time.  v_chunk/t_chunk form all the
+// derivatives of a chunk before the CPML and the updates: twelve in 3D, so 48
+// values (96 in FP64) are live at once and the capped kernels spill.  Here each
 // velocity component (and each shear stress, then the normal stresses and
 // the pressure) loads, differences, CPML-corrects and stores only what it
 // needs.  Every element goes through the same operations in the same order
 // as in v_tail/t_tail, so the results are bit-identical.
-// Which phases take this form, per precision (bit 0 = V, bit 1 = T).
-// Measured on B200 (192^3 and 552 x 552 x 424 order 2, 200^3 order 4):
-// COMP16 both (12-16 % off the step, its spills gone); FP64 the T phase (with
-// 2 CTAs per SM, 25-30 % off the step); FP32 neither (up to 10 % slower, its
-// latency-bound phases losing the loads they had in flight).
-#ifndef BP_SPLIT3_C16
-#define BP_SPLIT3_C16 3
+// Which phases take this form, per dimension and precision (bit 0 = V, bit 1
+// = T).  Measured on B200 (3D: 192^3 and 552 x 552 x 424 order 2, 200^3
+// order 4; 2D: 4040 x 2040 order 2): 3D COMP16 both (12-16 % off the step,
+// its spills gone); 2D COMP16 the T phase (13 % off it, the V phase 2 %
+// slower grouped); FP64 the 3D T phase (with 2 CTAs per SM, 25-30 % off the
+// 3D step); FP32 neither (10-20 % slower, its latency-bound phases losing the
+// loads they had in flight).
+#ifndef BP_GROUP3_C16
+#define BP_GROUP3_C16 3
 #endif
-#ifndef BP_SPLIT3_F32
-#define BP_SPLIT3_F32 0
+#ifndef BP_GROUP3_F32
+#define BP_GROUP3_F32 0
 #endif
-#ifndef BP_SPLIT3_F64
-#define BP_SPLIT3_F64 2
+#ifndef BP_GROUP3_F64
+#define BP_GROUP3_F64 2
 #endif
-template <class P, bool VPHASE>
-__host__ __device__ constexpr bool split3() {
-    return ((P::prec == BP_PREC_COMP16 ? BP_SPLIT3_C16 : P::prec == BP_PREC_FP32 ? BP_SPLIT3_F32 : BP_SPLIT3_F64) >>
-            (VPHASE ? 0 : 1)) & 1;
+#ifndef BP_GROUP2_C16
+#define BP_GROUP2_C16 2
+#endif
+#ifndef BP_GROUP2_F32
+#define BP_GROUP2_F32 0
+#endif
+#ifndef BP_GROUP2_F64
+#define BP_GROUP2_F64 0
+#endif
+template <int DIM, class P, bool VPHASE>
+__host__ __device__ constexpr bool grouped() {
+    const int m = DIM == 3 ? (P::prec == BP_PREC_COMP16 ? BP_GROUP3_C16 : P::prec == BP_PREC_FP32 ? BP_GROUP3_F32 : BP_GROUP3_F64)
+                           : (P::prec == BP_PREC_COMP16 ? BP_GROUP2_C16 : P::prec == BP_PREC_FP32 ? BP_GROUP2_F32 : BP_GROUP2_F64);
+    return (m >> (VPHASE ? 0 : 1)) & 1;
 }
 
 // Difference along x of one field at the chunk (span load), divided by H.
@@ -320,69 +336,74 @@ __device__ __forceinline__ void mask0(R (&d)[4], unsigned mask) {
         if (!(mask >> j & 1u)) d[j] = 0;
 }
 // CPML of one derivative on the slab of `axis` (slot k, half-grid profile if
-// half); nothing outside that slab.
-template <bool RS, class R>
-__device__ __forceinline__ void cpml3(const ShotDesc& S, void* const (&psi)[3], int axis, int k, bool half,
-                                      long long si, int x0, int y, int z, R (&d)[4], R r) {
+// half); nothing outside that slab.  Slabs hold 3 slots per phase in 2D, 4 in 3D.
+template <int DIM, bool RS, class R>
+__device__ __forceinline__ void cpml_g(const ShotDesc& S, void* const (&psi)[3], int axis, int k, bool half,
+                                       long long si, int x0, int y, int z, R (&d)[4], R r) {
     if (si < 0) return;
     const void* pb = half ? S.pb2[axis] : S.pb[axis];
     const void* pe = half ? S.pe2[axis] : S.pe[axis];
-    cpml_slot<4, RS, R>(d, psi[axis], S.slab_cells[axis], k, si, axis == 0, axis == 0 ? x0 : (axis == 1 ? y : z),
-                        x0, pb, pe, r);
+    cpml_slot<DIM == 3 ? 4 : 3, RS, R>(d, psi[axis], S.slab_cells[axis], k, si, axis == 0,
+                                        axis == 0 ? x0 : (axis == 1 ? y : z), x0, pb, pe, r);
 }
 
-// One velocity component AX (0 = x, 1 = y, 2 = z) of the 3D V phase
+// One velocity component AX (0 = x, 1 = y, 2 = z) of the V phase
 // (Float/main.cu:103-191 for that component).
-template <int ORD, class P, bool RS, int AX>
-__device__ __forceinline__ void v_comp3(const ShotDesc& S, long long c, long long row, int x0, int y, int z,
-                                        typename P::real r, unsigned mask, const typename P::real (&rf)[4]) {
+template <int DIM, int ORD, class P, bool RS, int AX>
+__device__ __forceinline__ void v_comp(const ShotDesc& S, long long c, long long row, int x0, int y, int z,
+                                       typename P::real r, unsigned mask, const typename P::real (&rf)[4]) {
     using R = typename P::real;
     const long long sy = S.pitch, sz = S.plane;
-    // dx, dy, dz: the stress derivatives summed into this component; dp: the
-    // pressure derivative along AX.  Slots as in v_tail.
+    // dx, dy, dz: the stress derivatives summed into this component (dy in 3D
+    // only); dp: the pressure derivative along AX.  Slots as in v_tail.
     R dx[4], dy[4], dz[4], dp[4];
     if constexpr (AX == 0) {
-        d_span<ORD, P, true>(S, BP_F_TXX, row, x0, dx);     // x1
-        d_rows<ORD, P, false>(S, BP_F_TXY, c, sy, dy);      // x2
-        d_rows<ORD, P, false>(S, BP_F_TXZ, c, sz, dz);      // x3
-        d_span<ORD, P, true>(S, BP_F_P, row, x0, dp);       // s1
+        d_span<ORD, P, true>(S, BP_F_TXX, row, x0, dx);                          // x1
+        if constexpr (DIM == 3) d_rows<ORD, P, false>(S, BP_F_TXY, c, sy, dy);   // x2
+        d_rows<ORD, P, false>(S, BP_F_TXZ, c, sz, dz);                           // x3
+        d_span<ORD, P, true>(S, BP_F_P, row, x0, dp);                            // s1
     } else if constexpr (AX == 1) {
-        d_span<ORD, P, false>(S, BP_F_TXY, row, x0, dx);    // y2
-        d_rows<ORD, P, true>(S, BP_F_TYY, c, sy, dy);       // y1
-        d_rows<ORD, P, false>(S, BP_F_TYZ, c, sz, dz);      // y3
-        d_rows<ORD, P, true>(S, BP_F_P, c, sy, dp);         // s2
+        d_span<ORD, P, false>(S, BP_F_TXY, row, x0, dx);                         // y2
+        d_rows<ORD, P, true>(S, BP_F_TYY, c, sy, dy);                            // y1
+        d_rows<ORD, P, false>(S, BP_F_TYZ, c, sz, dz);                           // y3
+        d_rows<ORD, P, true>(S, BP_F_P, c, sy, dp);                              // s2
     } else {
-        d_span<ORD, P, false>(S, BP_F_TXZ, row, x0, dx);    // z2
-        d_rows<ORD, P, false>(S, BP_F_TYZ, c, sy, dy);      // z3
-        d_rows<ORD, P, true>(S, BP_F_TZZ, c, sz, dz);       // z1
-        d_rows<ORD, P, true>(S, BP_F_P, c, sz, dp);         // s3
+        d_span<ORD, P, false>(S, BP_F_TXZ, row, x0, dx);                         // z2
+        if constexpr (DIM == 3) d_rows<ORD, P, false>(S, BP_F_TYZ, c, sy, dy);   // z3
+        d_rows<ORD, P, true>(S, BP_F_TZZ, c, sz, dz);                            // z1
+        d_rows<ORD, P, true>(S, BP_F_P, c, sz, dp);                              // s3
     }
-    if constexpr (P::prec == BP_PREC_COMP16 && RS) { scale4(dx, r); scale4(dy, r); scale4(dz, r); scale4(dp, r); }
-    mask0(dx, mask); mask0(dy, mask); mask0(dz, mask); mask0(dp, mask);
+    if constexpr (P::prec == BP_PREC_COMP16 && RS) {
+        scale4(dx, r); scale4(dz, r); scale4(dp, r);
+        if constexpr (DIM == 3) scale4(dy, r);
+    }
+    mask0(dx, mask); mask0(dz, mask); mask0(dp, mask);
+    if constexpr (DIM == 3) mask0(dy, mask);
     void* const psi[3] = {S.psiV[0], S.psiV[1], S.psiV[2]};
-    const long long s0 = slab_index(S, 0, x0, y, z), s1 = slab_index(S, 1, x0, y, z),
-                    s2 = slab_index(S, 2, x0, y, z);
+    const long long s0 = slab_index(S, 0, x0, y, z), s2 = slab_index(S, 2, x0, y, z);
+    const long long s1 = DIM == 3 ? slab_index(S, 1, x0, y, z) : -1;
     if constexpr (AX == 0) {
-        cpml3<RS>(S, psi, 0, 0, true, s0, x0, y, z, dx, r);
-        cpml3<RS>(S, psi, 0, 1, true, s0, x0, y, z, dp, r);
-        cpml3<RS>(S, psi, 1, 0, false, s1, x0, y, z, dy, r);
-        cpml3<RS>(S, psi, 2, 0, false, s2, x0, y, z, dz, r);
+        cpml_g<DIM, RS>(S, psi, 0, 0, true, s0, x0, y, z, dx, r);
+        cpml_g<DIM, RS>(S, psi, 0, 1, true, s0, x0, y, z, dp, r);
+        if constexpr (DIM == 3) cpml_g<DIM, RS>(S, psi, 1, 0, false, s1, x0, y, z, dy, r);
+        cpml_g<DIM, RS>(S, psi, 2, 0, false, s2, x0, y, z, dz, r);
     } else if constexpr (AX == 1) {
-        cpml3<RS>(S, psi, 0, 3, false, s0, x0, y, z, dx, r);
-        cpml3<RS>(S, psi, 1, 1, true, s1, x0, y, z, dy, r);
-        cpml3<RS>(S, psi, 1, 2, true, s1, x0, y, z, dp, r);
-        cpml3<RS>(S, psi, 2, 3, false, s2, x0, y, z, dz, r);
+        cpml_g<DIM, RS>(S, psi, 0, 3, false, s0, x0, y, z, dx, r);
+        cpml_g<DIM, RS>(S, psi, 1, 1, true, s1, x0, y, z, dy, r);
+        cpml_g<DIM, RS>(S, psi, 1, 2, true, s1, x0, y, z, dp, r);
+        cpml_g<DIM, RS>(S, psi, 2, 3, false, s2, x0, y, z, dz, r);
     } else {
-        cpml3<RS>(S, psi, 0, 2, false, s0, x0, y, z, dx, r);
-        cpml3<RS>(S, psi, 1, 3, false, s1, x0, y, z, dy, r);
-        cpml3<RS>(S, psi, 2, 1, true, s2, x0, y, z, dz, r);
-        cpml3<RS>(S, psi, 2, 2, true, s2, x0, y, z, dp, r);
+        cpml_g<DIM, RS>(S, psi, 0, 2, false, s0, x0, y, z, dx, r);
+        if constexpr (DIM == 3) cpml_g<DIM, RS>(S, psi, 1, 3, false, s1, x0, y, z, dy, r);
+        cpml_g<DIM, RS>(S, psi, 2, 1, true, s2, x0, y, z, dz, r);
+        cpml_g<DIM, RS>(S, psi, 2, 2, true, s2, x0, y, z, dp, r);
     }
-    // the divergence in v_tail's summation order: x1+x2+x3, y1+y2+y3, z1+z2+z3
+    // the divergence in v_tail's summation order: x1 (+x2) +x3, y1+y2+y3, z1+z2 (+z3)
     R sum[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-        if constexpr (AX == 0) sum[j] = dx[j] + dy[j] + dz[j];
+        if constexpr (DIM == 2) sum[j] = AX == 0 ? dx[j] + dz[j] : dz[j] + dx[j];
+        else if constexpr (AX == 0) sum[j] = dx[j] + dy[j] + dz[j];
         else if constexpr (AX == 1) sum[j] = dy[j] + dx[j] + dz[j];
         else sum[j] = dz[j] + dx[j] + dy[j];
     }
@@ -418,17 +439,17 @@ __device__ __forceinline__ void v_comp3(const ShotDesc& S, long long c, long lon
     P::st4(S.f[fu], S.flo[fu], c, nu);
 }
 
-template <int ORD, class P, bool RS>
-__device__ __forceinline__ void v_chunk3(const ShotDesc& S, int x0, int y, int z, typename P::real r,
-                                         unsigned mask) {
+template <int DIM, int ORD, class P, bool RS>
+__device__ __forceinline__ void v_chunk_g(const ShotDesc& S, int x0, int y, int z, typename P::real r,
+                                          unsigned mask) {
     using R = typename P::real;
     const long long c = x0 + (long long)y * S.pitch + (long long)z * S.plane;
     const long long row = c - x0;
     R rf[4];
     P::ld4(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, rf);
-    v_comp3<ORD, P, RS, 0>(S, c, row, x0, y, z, r, mask, rf);
-    v_comp3<ORD, P, RS, 1>(S, c, row, x0, y, z, r, mask, rf);
-    v_comp3<ORD, P, RS, 2>(S, c, row, x0, y, z, r, mask, rf);
+    v_comp<DIM, ORD, P, RS, 0>(S, c, row, x0, y, z, r, mask, rf);
+    if constexpr (DIM == 3) v_comp<DIM, ORD, P, RS, 1>(S, c, row, x0, y, z, r, mask, rf);
+    v_comp<DIM, ORD, P, RS, 2>(S, c, row, x0, y, z, r, mask, rf);
 }
 
 // Old value of a stress field at the chunk, with this step's rescale.
@@ -447,11 +468,11 @@ __device__ __forceinline__ void st_new(const ShotDesc& S, int f, long long c, un
     P::st4(S.f[f], S.flo[f], c, nv);
 }
 
-// One shear stress of the 3D T phase: SH 0 = txy, 1 = tyz, 2 = txz
+// One shear stress of the T phase: SH 0 = txy, 1 = tyz (3D only), 2 = txz
 // (Float/main.cu:232-294 for that stress).
-template <int ORD, class P, bool RS, int SH>
-__device__ __forceinline__ void t_shear3(const ShotDesc& S, long long c, long long row, int x0, int y, int z,
-                                         typename P::real r, unsigned mask, void* const (&psi)[3]) {
+template <int DIM, int ORD, class P, bool RS, int SH>
+__device__ __forceinline__ void t_shear(const ShotDesc& S, long long c, long long row, int x0, int y, int z,
+                                        typename P::real r, unsigned mask, void* const (&psi)[3]) {
     using R = typename P::real;
     const long long sy = S.pitch, sz = S.plane;
     R a[4], b[4];    // the two derivatives, in the order of the update's sum
@@ -467,14 +488,14 @@ __device__ __forceinline__ void t_shear3(const ShotDesc& S, long long c, long lo
     }
     mask0(a, mask); mask0(b, mask);
     if constexpr (SH == 0) {
-        cpml3<RS>(S, psi, 0, 3, true, slab_index(S, 0, x0, y, z), x0, y, z, b, r);
-        cpml3<RS>(S, psi, 1, 2, true, slab_index(S, 1, x0, y, z), x0, y, z, a, r);
+        cpml_g<DIM, RS>(S, psi, 0, 3, true, slab_index(S, 0, x0, y, z), x0, y, z, b, r);
+        cpml_g<DIM, RS>(S, psi, 1, 2, true, slab_index(S, 1, x0, y, z), x0, y, z, a, r);
     } else if constexpr (SH == 1) {
-        cpml3<RS>(S, psi, 1, 3, true, slab_index(S, 1, x0, y, z), x0, y, z, b, r);
-        cpml3<RS>(S, psi, 2, 3, true, slab_index(S, 2, x0, y, z), x0, y, z, a, r);
+        cpml_g<DIM, RS>(S, psi, 1, 3, true, slab_index(S, 1, x0, y, z), x0, y, z, b, r);
+        cpml_g<DIM, RS>(S, psi, 2, 3, true, slab_index(S, 2, x0, y, z), x0, y, z, a, r);
     } else {
-        cpml3<RS>(S, psi, 0, 2, true, slab_index(S, 0, x0, y, z), x0, y, z, b, r);
-        cpml3<RS>(S, psi, 2, 2, true, slab_index(S, 2, x0, y, z), x0, y, z, a, r);
+        cpml_g<DIM, RS>(S, psi, 0, 2, true, slab_index(S, 0, x0, y, z), x0, y, z, b, r);
+        cpml_g<DIM, RS>(S, psi, 2, 2, true, slab_index(S, 2, x0, y, z), x0, y, z, a, r);
     }
     constexpr int f = SH == 0 ? BP_F_TXY : SH == 1 ? BP_F_TYZ : BP_F_TXZ;
     constexpr int cm = SH == 0 ? TC_MUXY : SH == 1 ? TC_MUYZ : TC_MUXZ;
@@ -490,37 +511,44 @@ __device__ __forceinline__ void t_shear3(const ShotDesc& S, long long c, long lo
     st_new<P>(S, f, c, mask, n, o);
 }
 
-template <int ORD, class P, bool RS>
-__device__ __forceinline__ void t_chunk3(const ShotDesc& S, int x0, int y, int z, typename P::real r,
-                                         unsigned mask) {
+template <int DIM, int ORD, class P, bool RS>
+__device__ __forceinline__ void t_chunk_g(const ShotDesc& S, int x0, int y, int z, typename P::real r,
+                                          unsigned mask) {
     using R = typename P::real;
     const long long sy = S.pitch, sz = S.plane;
     const long long c = x0 + (long long)y * sy + (long long)z * sz;
     const long long row = c - x0;
     void* const psi[3] = {S.psiT[0], S.psiT[1], S.psiT[2]};
-    t_shear3<ORD, P, RS, 0>(S, c, row, x0, y, z, r, mask, psi);
-    t_shear3<ORD, P, RS, 1>(S, c, row, x0, y, z, r, mask, psi);
-    t_shear3<ORD, P, RS, 2>(S, c, row, x0, y, z, r, mask, psi);
+    if constexpr (DIM == 3) {
+        t_shear<DIM, ORD, P, RS, 0>(S, c, row, x0, y, z, r, mask, psi);
+        t_shear<DIM, ORD, P, RS, 1>(S, c, row, x0, y, z, r, mask, psi);
+    }
+    t_shear<DIM, ORD, P, RS, 2>(S, c, row, x0, y, z, r, mask, psi);
 
-    // normal stresses and pressure: the six divergence derivatives
+    // normal stresses and pressure: the divergence derivatives (uyy, wy in 3D)
     R uxx[4], uyy[4], uzz[4], wx[4], wy[4], wz[4];
     d_span<ORD, P, false>(S, BP_F_VUX, row, x0, uxx);
     d_span<ORD, P, false>(S, BP_F_VWX, row, x0, wx);
-    d_rows<ORD, P, false>(S, BP_F_VUY, c, sy, uyy);
-    d_rows<ORD, P, false>(S, BP_F_VWY, c, sy, wy);
+    if constexpr (DIM == 3) {
+        d_rows<ORD, P, false>(S, BP_F_VUY, c, sy, uyy);
+        d_rows<ORD, P, false>(S, BP_F_VWY, c, sy, wy);
+    }
     d_rows<ORD, P, false>(S, BP_F_VUZ, c, sz, uzz);
     d_rows<ORD, P, false>(S, BP_F_VWZ, c, sz, wz);
-    mask0(uxx, mask); mask0(wx, mask); mask0(uyy, mask); mask0(wy, mask); mask0(uzz, mask); mask0(wz, mask);
+    mask0(uxx, mask); mask0(wx, mask); mask0(uzz, mask); mask0(wz, mask);
+    if constexpr (DIM == 3) { mask0(uyy, mask); mask0(wy, mask); }
     {
         const long long s0 = slab_index(S, 0, x0, y, z);
-        cpml3<RS>(S, psi, 0, 0, false, s0, x0, y, z, uxx, r);
-        cpml3<RS>(S, psi, 0, 1, false, s0, x0, y, z, wx, r);
-        const long long s1 = slab_index(S, 1, x0, y, z);
-        cpml3<RS>(S, psi, 1, 0, false, s1, x0, y, z, uyy, r);
-        cpml3<RS>(S, psi, 1, 1, false, s1, x0, y, z, wy, r);
+        cpml_g<DIM, RS>(S, psi, 0, 0, false, s0, x0, y, z, uxx, r);
+        cpml_g<DIM, RS>(S, psi, 0, 1, false, s0, x0, y, z, wx, r);
+        if constexpr (DIM == 3) {
+            const long long s1 = slab_index(S, 1, x0, y, z);
+            cpml_g<DIM, RS>(S, psi, 1, 0, false, s1, x0, y, z, uyy, r);
+            cpml_g<DIM, RS>(S, psi, 1, 1, false, s1, x0, y, z, wy, r);
+        }
         const long long s2 = slab_index(S, 2, x0, y, z);
-        cpml3<RS>(S, psi, 2, 0, false, s2, x0, y, z, uzz, r);
-        cpml3<RS>(S, psi, 2, 1, false, s2, x0, y, z, wz, r);
+        cpml_g<DIM, RS>(S, psi, 2, 0, false, s2, x0, y, z, uzz, r);
+        cpml_g<DIM, RS>(S, psi, 2, 1, false, s2, x0, y, z, wz, r);
     }
     R cC[4], cM[4], cH[4], cH2[4], o[4], n[4];
     const R dt = S.dtr<R>();
@@ -529,10 +557,17 @@ __device__ __forceinline__ void t_chunk3(const ShotDesc& S, int x0, int y, int z
     ld_old<P, RS>(S, BP_F_P, c, r, o);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-        if constexpr (P::prec == BP_PREC_COMP16)
-            n[j] = o[j] - cC[j] * (uxx[j] + uyy[j] + uzz[j]) - cM[j] * (wx[j] + wy[j] + wz[j]);
-        else
-            n[j] = o[j] - dt * (cC[j] * (uxx[j] + uyy[j] + uzz[j]) + cM[j] * (wx[j] + wy[j] + wz[j]));
+        if constexpr (DIM == 3) {
+            if constexpr (P::prec == BP_PREC_COMP16)
+                n[j] = o[j] - cC[j] * (uxx[j] + uyy[j] + uzz[j]) - cM[j] * (wx[j] + wy[j] + wz[j]);
+            else
+                n[j] = o[j] - dt * (cC[j] * (uxx[j] + uyy[j] + uzz[j]) + cM[j] * (wx[j] + wy[j] + wz[j]));
+        } else {
+            if constexpr (P::prec == BP_PREC_COMP16)
+                n[j] = o[j] - cC[j] * (uxx[j] + uzz[j]) - cM[j] * (wx[j] + wz[j]);
+            else
+                n[j] = o[j] - dt * (cC[j] * (uxx[j] + uzz[j]) + cM[j] * (wx[j] + wz[j]));
+        }
     }
     st_new<P>(S, BP_F_P, c, mask, n, o);
     P::ld4(S.tc[TC_H], S.tclo[TC_H], c, cH);
@@ -540,28 +575,44 @@ __device__ __forceinline__ void t_chunk3(const ShotDesc& S, int x0, int y, int z
     ld_old<P, RS>(S, BP_F_TXX, c, r, o);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-        if constexpr (P::prec == BP_PREC_COMP16)
-            n[j] = o[j] + cH2[j] * (uyy[j] + uzz[j]) + cH[j] * uxx[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
-        else
-            n[j] = o[j] + dt * (cH2[j] * (uyy[j] + uzz[j]) + cH[j] * uxx[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
+        if constexpr (DIM == 3) {
+            if constexpr (P::prec == BP_PREC_COMP16)
+                n[j] = o[j] + cH2[j] * (uyy[j] + uzz[j]) + cH[j] * uxx[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
+            else
+                n[j] = o[j] + dt * (cH2[j] * (uyy[j] + uzz[j]) + cH[j] * uxx[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
+        } else {
+            if constexpr (P::prec == BP_PREC_COMP16)
+                n[j] = o[j] + cH2[j] * uzz[j] + cH[j] * uxx[j] + cC[j] * (wx[j] + wz[j]);
+            else
+                n[j] = o[j] + dt * (cH2[j] * uzz[j] + cH[j] * uxx[j] + cC[j] * (wx[j] + wz[j]));
+        }
     }
     st_new<P>(S, BP_F_TXX, c, mask, n, o);
-    ld_old<P, RS>(S, BP_F_TYY, c, r, o);
+    if constexpr (DIM == 3) {
+        ld_old<P, RS>(S, BP_F_TYY, c, r, o);
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-        if constexpr (P::prec == BP_PREC_COMP16)
-            n[j] = o[j] + cH2[j] * (uxx[j] + uzz[j]) + cH[j] * uyy[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
-        else
-            n[j] = o[j] + dt * (cH2[j] * (uxx[j] + uzz[j]) + cH[j] * uyy[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
+        for (int j = 0; j < 4; j++) {
+            if constexpr (P::prec == BP_PREC_COMP16)
+                n[j] = o[j] + cH2[j] * (uxx[j] + uzz[j]) + cH[j] * uyy[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
+            else
+                n[j] = o[j] + dt * (cH2[j] * (uxx[j] + uzz[j]) + cH[j] * uyy[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
+        }
+        st_new<P>(S, BP_F_TYY, c, mask, n, o);
     }
-    st_new<P>(S, BP_F_TYY, c, mask, n, o);
     ld_old<P, RS>(S, BP_F_TZZ, c, r, o);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-        if constexpr (P::prec == BP_PREC_COMP16)
-            n[j] = o[j] + cH2[j] * (uxx[j] + uyy[j]) + cH[j] * uzz[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
-        else
-            n[j] = o[j] + dt * (cH2[j] * (uxx[j] + uyy[j]) + cH[j] * uzz[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
+        if constexpr (DIM == 3) {
+            if constexpr (P::prec == BP_PREC_COMP16)
+                n[j] = o[j] + cH2[j] * (uxx[j] + uyy[j]) + cH[j] * uzz[j] + cC[j] * (wx[j] + wy[j] + wz[j]);
+            else
+                n[j] = o[j] + dt * (cH2[j] * (uxx[j] + uyy[j]) + cH[j] * uzz[j] + cC[j] * (wx[j] + wy[j] + wz[j]));
+        } else {
+            if constexpr (P::prec == BP_PREC_COMP16)
+                n[j] = o[j] + cH2[j] * uxx[j] + cH[j] * uzz[j] + cC[j] * (wx[j] + wz[j]);
+            else
+                n[j] = o[j] + dt * (cH2[j] * uxx[j] + cH[j] * uzz[j] + cC[j] * (wx[j] + wz[j]));
+        }
     }
     st_new<P>(S, BP_F_TZZ, c, mask, n, o);
 }
@@ -638,13 +689,13 @@ __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHAS
         // COMP16: the rescale products only on the steps whose factor is not
         // exactly 1 (a uniform branch; the products are never fused, so both
         // forms give the same bits when r == 1)
-        if constexpr (DIM == 3 && split3<P, VPHASE>()) {
+        if constexpr (grouped<DIM, P, VPHASE>()) {
             if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
-                if constexpr (VPHASE) v_chunk3<ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
-                else t_chunk3<ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+                if constexpr (VPHASE) v_chunk_g<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+                else t_chunk_g<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
             } else {
-                if constexpr (VPHASE) v_chunk3<ORD, P, false>(S, x0, y, z, r, mask);
-                else t_chunk3<ORD, P, false>(S, x0, y, z, r, mask);
+                if constexpr (VPHASE) v_chunk_g<DIM, ORD, P, false>(S, x0, y, z, r, mask);
+                else t_chunk_g<DIM, ORD, P, false>(S, x0, y, z, r, mask);
             }
         } else if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
             if constexpr (VPHASE) v_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
