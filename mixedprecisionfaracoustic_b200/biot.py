@@ -209,12 +209,19 @@ class Simulation:
         check(self.lib.bp_get_dims(self.h, C.byref(x), C.byref(y), C.byref(z)), "bp_get_dims")
         return x.value, y.value, z.value
 
-    def traces(self, comp) -> np.ndarray:
-        """(nrec, nt) float32 seismogram of component 'txx','tzz','vux','vwx','p'."""
+    def traces(self, comp, out: np.ndarray = None) -> np.ndarray:
+        """(nrec, nt) float32 seismogram of component 'txx','tzz','vux','vwx','p'.
+
+        out: a C-contiguous float32 array of nrec * nt elements to fill (for
+        instance pinned host memory, which the copy reaches at full speed);
+        a new array otherwise."""
         ci = _abi.TRACE[comp] if isinstance(comp, str) else int(comp)
-        out = np.zeros((self.cfg.nrec, self.cfg.nt), dtype=np.float32)
+        if out is None:
+            out = np.zeros((self.cfg.nrec, self.cfg.nt), dtype=np.float32)
+        elif out.dtype != np.float32 or not out.flags.c_contiguous or out.size != self.cfg.nrec * self.cfg.nt:
+            raise ValueError("out must be a C-contiguous float32 array of nrec * nt elements")
         check(self.lib.bp_get_traces(self.h, ci, fptr(out), out.size), "bp_get_traces")
-        return out
+        return out.reshape(self.cfg.nrec, self.cfg.nt)
 
     def snapshot(self, k: int, fld: str) -> np.ndarray:
         n = C.c_size_t()

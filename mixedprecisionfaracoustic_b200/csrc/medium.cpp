@@ -3,9 +3,12 @@
 // bp_medium_reference_borehole restates the reference's create_model
 // (Float/main.cu:1590-1655) with its exact float/double promotions, so the
 // drop-in run sees the same cell-centred Biot coefficients as the reference.
+#include <algorithm>
 #include <cmath>
 #include <cstddef>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "../../include/biot.h"
 
@@ -103,10 +106,37 @@ int bp_cfl_limit(const bp_config* cfg, const bp_medium* m, double* dt_max, doubl
         return BP_ERR_ARG;
     }
     const size_t n = (size_t)cfg->nx * (cfg->dim == 3 ? cfg->ny : 1) * cfg->nz;
+    // The scan runs on host threads in contiguous ranges; a cell whose six
+    // inputs equal the previous cell's reuses its velocity (layered and
+    // blocky media repeat along x), which changes no result.
+    auto scan = [m](size_t lo, size_t hi) {
+        double vmax = 0, v = 0;
+        float last[6] = {NAN, NAN, NAN, NAN, NAN, NAN};
+        for (size_t i = lo; i < hi; i++) {
+            const float in[6] = {m->rho[i], m->rhof[i], m->M[i], m->C[i], m->H[i], m->C2[i]};
+            if (!(in[0] == last[0] && in[1] == last[1] && in[2] == last[2] && in[3] == last[3] &&
+                  in[4] == last[4] && in[5] == last[5])) {
+                v = cell_vmax(in[0], in[1], in[2], in[3], in[4], in[5]);
+                std::copy(in, in + 6, last);
+            }
+            if (v > vmax) vmax = v;
+        }
+        return vmax;
+    };
+    const size_t chunk = (size_t)1 << 18;
+    const int nthr = (int)std::min<size_t>(std::max(1u, std::min(std::thread::hardware_concurrency(), 32u)),
+                                           (n + chunk - 1) / chunk);
     double vmax = 0;
-    for (size_t i = 0; i < n; i++) {
-        const double v = cell_vmax(m->rho[i], m->rhof[i], m->M[i], m->C[i], m->H[i], m->C2[i]);
-        if (v > vmax) vmax = v;
+    if (nthr <= 1) {
+        vmax = scan(0, n);
+    } else {
+        std::vector<double> part(nthr, 0.0);
+        std::vector<std::thread> pool;
+        const size_t per = (n + nthr - 1) / nthr;
+        for (int t = 0; t < nthr; t++)
+            pool.emplace_back([&, t] { part[t] = scan(std::min(n, t * per), std::min(n, (t + 1) * per)); });
+        for (auto& th : pool) th.join();
+        vmax = *std::max_element(part.begin(), part.end());
     }
     const double stencil = cfg->order == 4 ? (9.0 / 8.0 + 1.0 / 24.0) : 1.0;
     *dt_max = vmax > 0 ? cfg->dx / (vmax * std::sqrt((double)cfg->dim) * stencil) : 1e30;

@@ -8,7 +8,7 @@ import pytest
 
 from conftest import ROOT, has_gpu
 from mixedprecisionfaracoustic_b200 import _abi
-from mixedprecisionfaracoustic_b200.biot import ShotConfig, biot_from_moduli, cfl_limit, reference_borehole_medium
+from mixedprecisionfaracoustic_b200.biot import Medium, ShotConfig, biot_from_moduli, cfl_limit, reference_borehole_medium
 from mixedprecisionfaracoustic_b200.presets import c0_coefficients, config0, config1, reference_compat
 from oracle import oracle as O
 
@@ -94,6 +94,38 @@ def test_cfl_limits():
     if not has_gpu():
         rc, _ = _create(cfg, med)
         assert rc in (_abi.BP_ERR_CFL, _abi.BP_ERR_NO_DEVICE)
+
+
+def _vmax_numpy(med):
+    """Fast P velocity bound of every cell (the largest root of the Biot
+    dispersion determinant, or sqrt(H / rho) for a singular mass matrix)."""
+    rho, rhof, M, C, H, C2 = (np.asarray(med[k], dtype=np.float64).ravel() for k in ("rho", "rhof", "M", "C", "H", "C2"))
+    v2 = np.where(rho > 0, H / rho, 0.0)
+    a = rho * C2 - rhof * rhof
+    b = -(H * C2 + M * rho - 2 * C * rhof)
+    c = H * M - C * C
+    with np.errstate(all="ignore"):
+        root = (-b + np.sqrt(np.maximum(b * b - 4 * a * c, 0))) / (2 * a)
+    v2 = np.where((a > 1e-9 * np.abs(rho * C2)) & (root > v2), root, v2)
+    return float(np.sqrt(np.maximum(v2, 0)).max())
+
+
+def test_cfl_scan_on_threads_matches_every_cell():
+    """The threaded scan with reuse of repeated cells finds the same maximum
+    as an evaluation of every cell: a layered medium (runs of equal cells) with
+    its fastest cell alone in the middle of a run, over several scan ranges."""
+    cfg, med = config0(n=16, npml=4, nt=10, nrec=8)
+    nx, nz = 1500, 1100                      # 1.65 M cells: several 2^18-cell ranges
+    cfg.dim, cfg.nx, cfg.ny, cfg.nz = 2, nx, 1, nz
+    rng = np.random.default_rng(7)
+    layers = rng.integers(0, 4, nz)
+    lay = {k: np.asarray(v, dtype=np.float32).ravel()[:4] for k, v in med.items()}
+    m = Medium({k: np.ascontiguousarray(np.repeat(v[layers][:, None], nx, axis=1)) for k, v in lay.items()})
+    base = _vmax_numpy(m)
+    m["H"][nz // 2, nx // 3] *= np.float32(1.7)        # one fast cell
+    dt, v = cfl_limit(cfg, m)
+    assert v == pytest.approx(_vmax_numpy(m), rel=1e-12)
+    assert v > 1.05 * base
 
 
 def test_struct_layout_matches_header(tmp_path):

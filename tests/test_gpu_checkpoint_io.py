@@ -125,3 +125,23 @@ def test_streamed_trace_windows_equal_the_final_traces():
         full = s.traces("vux")
     got = np.concatenate([pinned[i][:, :min(win, cfg.nt - i * win)] for i in range(k)], axis=1)
     assert np.array_equal(got[umap], full)
+
+
+def test_traces_into_caller_buffers():
+    """traces(c, out=...) fills a caller's buffer (pinned host memory here)
+    with the same values, and refuses a buffer of the wrong size or type."""
+    import torch
+    cfg, med = case("2d", "fp32")
+    with Simulation(cfg, med) as s:
+        s.run(cfg.nt)
+        s.sync()
+        for c in _abi.TRACES:
+            buf = torch.empty(cfg.nrec * cfg.nt, dtype=torch.float32, pin_memory=True).numpy()
+            got = s.traces(c, out=buf)
+            assert got.shape == (cfg.nrec, cfg.nt)
+            assert np.shares_memory(got, buf)
+            assert np.array_equal(got, s.traces(c))
+        with pytest.raises(ValueError):
+            s.traces("txx", out=np.zeros(cfg.nrec * cfg.nt - 1, dtype=np.float32))
+        with pytest.raises(ValueError):
+            s.traces("txx", out=np.zeros(cfg.nrec * cfg.nt, dtype=np.float64))
