@@ -253,11 +253,8 @@ int bp_batch_get_traces(bp_batch* b, int shot, int comp, float* host, size_t n) 
     const size_t nt = sh.cfg.nt, nr = sh.cfg.nrec;
     if (n < nr * nt) { set_error("host buffer too small"); return BP_ERR_ARG; }
     cudaError_t e = cudaStreamSynchronize(b->st);
-    std::vector<float> u((size_t)sh.nurec * nt);
-    if (e == cudaSuccess && !u.empty())
-        e = cudaMemcpy(u.data(), sh.desc.traces + (size_t)comp * sh.nurec * nt, u.size() * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = sh.copy_traces(comp, host);
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
-    for (size_t r = 0; r < nr; r++) std::memcpy(host + r * nt, u.data() + (size_t)sh.urec_of[r] * nt, nt * 4);
     return BP_OK;
 }
 

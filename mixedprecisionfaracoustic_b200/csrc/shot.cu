@@ -569,6 +569,24 @@ int Shot::blowup_step(cudaStream_t st) const {
     return h;
 }
 
+cudaError_t Shot::copy_traces(int comp, float* host) const {
+    const size_t nt = cfg.nt, nr = cfg.nrec;
+    const float* src = desc.traces + (size_t)comp * nurec * nt;
+    // receivers all distinct and in order (the usual case): one copy straight
+    // into the caller's buffer, at full speed when that buffer is pinned
+    bool identity = (size_t)nurec == nr;
+    for (size_t r = 0; identity && r < nr; r++) identity = (size_t)urec_of[r] == r;
+    if (identity) return nr ? cudaMemcpy(host, src, nr * nt * 4, cudaMemcpyDeviceToHost) : cudaSuccess;
+    // receivers sharing a cell: the unique traces, then one row per receiver
+    std::vector<float> u((size_t)nurec * nt);
+    if (!u.empty()) {
+        const cudaError_t e = cudaMemcpy(u.data(), src, u.size() * 4, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return e;
+    }
+    for (size_t r = 0; r < nr; r++) std::memcpy(host + r * nt, u.data() + (size_t)urec_of[r] * nt, nt * 4);
+    return cudaSuccess;
+}
+
 void Shot::destroy() {
     if (arena) arena_release(arena, arena_alloc_bytes);
     arena = nullptr;

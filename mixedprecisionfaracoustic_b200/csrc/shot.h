@@ -95,6 +95,9 @@ struct Shot {
     // 1 + the first step whose recorded receiver values were not all finite,
     // 0 if none (synchronises st).
     int blowup_step(cudaStream_t st) const;
+    // Seismogram component comp of every receiver (receiver order, nrec x nt)
+    // into host memory; the caller has synchronised the shot's stream.
+    cudaError_t copy_traces(int comp, float* host) const;
 
     // Computes the arena size for cfg without allocating (admission control).
     static int plan_bytes(const bp_config* cfg, size_t* bytes);

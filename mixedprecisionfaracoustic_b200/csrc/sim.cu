@@ -218,10 +218,7 @@ int bp_get_traces(bp_sim* s, int comp, float* host, size_t n) {
     const size_t nt = sh.cfg.nt, nr = sh.cfg.nrec;
     if (n < nr * nt) { set_error("host buffer too small"); return BP_ERR_ARG; }
     SIM_CK(cudaStreamSynchronize(s->st));
-    std::vector<float> u((size_t)sh.nurec * nt);
-    if (!u.empty())
-        SIM_CK(cudaMemcpy(u.data(), sh.desc.traces + (size_t)comp * sh.nurec * nt, u.size() * 4, cudaMemcpyDeviceToHost));
-    for (size_t r = 0; r < nr; r++) std::memcpy(host + r * nt, u.data() + (size_t)sh.urec_of[r] * nt, nt * 4);
+    SIM_CK(sh.copy_traces(comp, host));
     return BP_OK;
 }
 

@@ -89,3 +89,23 @@ def test_no_receivers_and_no_source():
         for f in ("vux", "vwz", "p", "txx", "txz"):
             assert np.abs(s.field(f)).max() == 0, f
         assert np.abs(s.traces("p")).max() == 0
+
+
+def test_receivers_sharing_cells_and_out_of_order():
+    """Receivers listed out of order and several on one cell each get that
+    cell's seismogram: the same rows as a run with the distinct cells in order."""
+    cfg, med = shot(2, (64, 1, 48), npml=8, nrec=6)
+    order = [3, 0, 3, 5, 1, 0, 2, 4, 3]
+    dup = shot(2, (64, 1, 48), npml=8, nrec=6)[0]
+    dup.rec_x = [cfg.rec_x[i] for i in order]
+    dup.rec_y = [cfg.rec_y[i] for i in order]
+    dup.rec_z = [cfg.rec_z[i] for i in order]
+    with Simulation(cfg, med) as a, Simulation(dup, med) as b:
+        a.run(cfg.nt)
+        b.run(cfg.nt)
+        a.sync()
+        b.sync()
+        for c in _abi.TRACES:
+            ta, tb = a.traces(c), b.traces(c)
+            assert tb.shape == (len(order), cfg.nt)
+            assert np.array_equal(tb, ta[order]), c
