@@ -321,8 +321,11 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
 
     // ---- medium upload (transient) ----
     const size_t pn = (size_t)c->nx * (dim == 3 ? c->ny : 1) * c->nz;
+    // the staging block comes from the arena cache, like the arena itself, so
+    // a create after a destroy of similar size allocates nothing
     float* stage = nullptr;
-    BP_CK(cudaMalloc(&stage, 9 * pn * sizeof(float)));
+    size_t stage_bytes = 0;
+    BP_CK(arena_alloc(9 * pn * sizeof(float), (void**)&stage, &stage_bytes));
     const float* src9[9] = {med->rho, med->rhof, med->M, med->C, med->H, med->H2mu, med->mu, med->C1, med->C2};
     const float* dm[9];
     int rc2 = BP_OK;
@@ -331,7 +334,7 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
         cudaError_t e = cudaMemcpyAsync((void*)dm[k], src9[k], pn * sizeof(float), cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) { set_error(std::string("medium upload: ") + cudaGetErrorString(e)); rc2 = BP_ERR_CUDA; }
     }
-    auto fail = [&](int code) { cudaStreamSynchronize(st); cudaFree(stage); return code; };
+    auto fail = [&](int code) { cudaStreamSynchronize(st); arena_release(stage, stage_bytes); return code; };
     if (rc2) return fail(rc2);
 
     // ---- CPML profiles, FP64 ----
@@ -412,7 +415,7 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     // the first source sample, injected before the first V phase (Float/main.cu:1055-1062)
     if (e == cudaSuccess) e = launch_inject(c->precision, d_desc, 1, 0, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(stage);
+    arena_release(stage, stage_bytes);
     if (e != cudaSuccess) { set_error(std::string("shot set-up: ") + cudaGetErrorString(e)); return BP_ERR_CUDA; }
 
     long long cx = p.nx - 2 * S.hw, cz = p.nz - 2 * S.hw, cy = dim == 3 ? p.ny - 2 * S.hw : 1;
