@@ -133,7 +133,11 @@ typedef struct bp_sim bp_sim;
 /* Replaces main() setup, Float/main.cu:300-1040 (medium padding, staggered
  * averaging, CPML profiles, 93 cudaMalloc + H2D copies) and, for COMP16, the
  * exponent-scaling precompute of Half/main.cu:745-1045.  Copies the medium to
- * the device, runs the FP64 precompute kernels and leaves the state at it=0. */
+ * the device, runs the FP64 precompute kernels and leaves the state at it=0.
+ * The padded grid (row pitch x ny x nz, the pitch being nx + 2 npml rounded up
+ * to 32) must hold fewer than 2^31 cells, else BP_ERR_ARG: the kernels address
+ * cells with 32-bit offsets.  (At FP32 or FP64 a larger grid would not fit in
+ * a B200's memory anyway.) */
 int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out);
 
 /* Replaces the time loop body, Float/main.cu:1048-1164: for each of nsteps

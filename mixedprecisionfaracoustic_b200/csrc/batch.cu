@@ -33,11 +33,16 @@ long long BatchCore::total_cells() const {
 int BatchCore::rebuild() {
     const int n = (int)shots.size();
     if (n > d_cap) {
-        if (d_descs) cudaFree(d_descs);
+        // descriptor blocks come from the arena cache (no cudaMalloc/cudaFree
+        // per batch); the old one goes back once no launch can still read it
+        if (d_descs) {
+            if (st) cudaStreamSynchronize(st);
+            arena_release(d_descs, d_bytes);
+        }
         d_descs = nullptr;
         d_cap = std::max(n, 2 * d_cap);
-        cudaError_t e = cudaMalloc(&d_descs, (size_t)d_cap * sizeof(ShotDesc));
-        if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); d_cap = 0; return BP_ERR_OOM; }
+        cudaError_t e = arena_alloc((size_t)d_cap * sizeof(ShotDesc), (void**)&d_descs, &d_bytes);
+        if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); d_descs = nullptr; d_cap = 0; return BP_ERR_OOM; }
     }
     std::vector<ShotDesc> h(n);
     long long t0 = 0;
@@ -148,7 +153,7 @@ void BatchCore::release() {
     run.reset_graph();
     for (auto& s : shots) s->destroy();
     shots.clear();
-    if (d_descs) cudaFree(d_descs);
+    if (d_descs) arena_release(d_descs, d_bytes);
     d_descs = nullptr;
     d_cap = 0;
 }

@@ -30,6 +30,7 @@ struct BatchCore {
     std::vector<std::unique_ptr<Shot>> shots;   // resident shots
     ShotDesc* d_descs = nullptr;
     int d_cap = 0;
+    size_t d_bytes = 0;                // block size of d_descs (from the arena cache)
     Runner run;
     int ctas_per_sm = 0, steps_per_sync = 0;    // 0 = autotune
     bool tuned = false;

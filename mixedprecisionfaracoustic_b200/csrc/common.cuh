@@ -41,6 +41,13 @@ struct Slab {
     }
 };
 
+// Offset of a cell (or of a slab memory variable) within one array.  Every
+// array of a shot holds fewer than 2^31 elements (validate_config bounds the
+// padded grid), so the phase kernels index with 32-bit integers: one
+// wide multiply-add forms each address, where 64-bit offsets cost several
+// instructions per access (1-5 % of the step, measured on B200).
+using cidx = int;
+
 struct ShotDesc {
     int dim, order, hw;           // hw = order / 2 = untouched border cells
     int nx, ny, nz;               // padded extents
@@ -142,26 +149,26 @@ __device__ __forceinline__ void encode_ch(float v, __half& hi, int8_t& lo) {
 struct PolF32 {
     using real = float;
     static constexpr int prec = BP_PREC_FP32;
-    __device__ __forceinline__ static void ld4(const void* p, const int8_t*, long long i, real (&v)[4]) {
+    __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
         float4 t = *reinterpret_cast<const float4*>(static_cast<const float*>(p) + i);
         v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
     }
-    __device__ __forceinline__ static real ld1(const void* p, const int8_t*, long long i) {
+    __device__ __forceinline__ static real ld1(const void* p, const int8_t*, cidx i) {
         return static_cast<const float*>(p)[i];
     }
-    __device__ __forceinline__ static void st4(void* p, int8_t*, long long i, const real (&v)[4]) {
+    __device__ __forceinline__ static void st4(void* p, int8_t*, cidx i, const real (&v)[4]) {
         *reinterpret_cast<float4*>(static_cast<float*>(p) + i) = make_float4(v[0], v[1], v[2], v[3]);
     }
-    __device__ __forceinline__ static void st1(void* p, int8_t*, long long i, real v) {
+    __device__ __forceinline__ static void st1(void* p, int8_t*, cidx i, real v) {
         static_cast<float*>(p)[i] = v;
     }
     // raw (undecoded) loads, for kernels that issue loads well before use
     using raw4 = float4;
     using raw1 = float;
-    __device__ __forceinline__ static raw4 ldr4(const void* p, const int8_t*, long long i) {
+    __device__ __forceinline__ static raw4 ldr4(const void* p, const int8_t*, cidx i) {
         return *reinterpret_cast<const float4*>(static_cast<const float*>(p) + i);
     }
-    __device__ __forceinline__ static raw1 ldr1(const void* p, const int8_t*, long long i) {
+    __device__ __forceinline__ static raw1 ldr1(const void* p, const int8_t*, cidx i) {
         return static_cast<const float*>(p)[i];
     }
     __device__ __forceinline__ static raw4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.f); }
@@ -175,29 +182,29 @@ struct PolF32 {
 struct PolF64 {
     using real = double;
     static constexpr int prec = BP_PREC_FP64;
-    __device__ __forceinline__ static void ld4(const void* p, const int8_t*, long long i, real (&v)[4]) {
+    __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
         const double2* q = reinterpret_cast<const double2*>(static_cast<const double*>(p) + i);
         double2 a = q[0], b = q[1];
         v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
     }
-    __device__ __forceinline__ static real ld1(const void* p, const int8_t*, long long i) {
+    __device__ __forceinline__ static real ld1(const void* p, const int8_t*, cidx i) {
         return static_cast<const double*>(p)[i];
     }
-    __device__ __forceinline__ static void st4(void* p, int8_t*, long long i, const real (&v)[4]) {
+    __device__ __forceinline__ static void st4(void* p, int8_t*, cidx i, const real (&v)[4]) {
         double2* q = reinterpret_cast<double2*>(static_cast<double*>(p) + i);
         q[0] = make_double2(v[0], v[1]);
         q[1] = make_double2(v[2], v[3]);
     }
-    __device__ __forceinline__ static void st1(void* p, int8_t*, long long i, real v) {
+    __device__ __forceinline__ static void st1(void* p, int8_t*, cidx i, real v) {
         static_cast<double*>(p)[i] = v;
     }
     struct raw4 { double2 a, b; };
     using raw1 = double;
-    __device__ __forceinline__ static raw4 ldr4(const void* p, const int8_t*, long long i) {
+    __device__ __forceinline__ static raw4 ldr4(const void* p, const int8_t*, cidx i) {
         const double2* q = reinterpret_cast<const double2*>(static_cast<const double*>(p) + i);
         return raw4{q[0], q[1]};
     }
-    __device__ __forceinline__ static raw1 ldr1(const void* p, const int8_t*, long long i) {
+    __device__ __forceinline__ static raw1 ldr1(const void* p, const int8_t*, cidx i) {
         return static_cast<const double*>(p)[i];
     }
     __device__ __forceinline__ static raw4 zero4() { return raw4{make_double2(0, 0), make_double2(0, 0)}; }
@@ -213,7 +220,7 @@ struct PolF64 {
 struct PolC16 {
     using real = float;
     static constexpr int prec = BP_PREC_COMP16;
-    __device__ __forceinline__ static void ld4(const void* p, const int8_t* lo, long long i, real (&v)[4]) {
+    __device__ __forceinline__ static void ld4(const void* p, const int8_t* lo, cidx i, real (&v)[4]) {
         uint2 h = *reinterpret_cast<const uint2*>(static_cast<const __half*>(p) + i);
         __half2 h01 = *reinterpret_cast<__half2*>(&h.x);
         __half2 h23 = *reinterpret_cast<__half2*>(&h.y);
@@ -227,11 +234,11 @@ struct PolC16 {
             for (int j = 0; j < 4; j++) v[j] = __half2float(hs[j]);
         }
     }
-    __device__ __forceinline__ static real ld1(const void* p, const int8_t* lo, long long i) {
+    __device__ __forceinline__ static real ld1(const void* p, const int8_t* lo, cidx i) {
         __half h = static_cast<const __half*>(p)[i];
         return lo ? decode_ch(h, lo[i]) : __half2float(h);
     }
-    __device__ __forceinline__ static void st4(void* p, int8_t* lo, long long i, const real (&v)[4]) {
+    __device__ __forceinline__ static void st4(void* p, int8_t* lo, cidx i, const real (&v)[4]) {
         __half hs[4];
         int8_t ls[4];
 #pragma unroll
@@ -243,7 +250,7 @@ struct PolC16 {
         *reinterpret_cast<uint2*>(static_cast<__half*>(p) + i) = h;
         *reinterpret_cast<char4*>(lo + i) = make_char4(ls[0], ls[1], ls[2], ls[3]);
     }
-    __device__ __forceinline__ static void st1(void* p, int8_t* lo, long long i, real v) {
+    __device__ __forceinline__ static void st1(void* p, int8_t* lo, cidx i, real v) {
         __half h;
         int8_t l;
         encode_ch(v, h, l);
@@ -254,13 +261,13 @@ struct PolC16 {
     // the array has none, which decodes to the same value as hi alone)
     struct raw4 { uint2 h; char4 l; };
     struct raw1 { __half h; int8_t l; };
-    __device__ __forceinline__ static raw4 ldr4(const void* p, const int8_t* lo, long long i) {
+    __device__ __forceinline__ static raw4 ldr4(const void* p, const int8_t* lo, cidx i) {
         raw4 t;
         t.h = *reinterpret_cast<const uint2*>(static_cast<const __half*>(p) + i);
         t.l = lo ? *reinterpret_cast<const char4*>(lo + i) : make_char4(0, 0, 0, 0);
         return t;
     }
-    __device__ __forceinline__ static raw1 ldr1(const void* p, const int8_t* lo, long long i) {
+    __device__ __forceinline__ static raw1 ldr1(const void* p, const int8_t* lo, cidx i) {
         raw1 t;
         t.h = static_cast<const __half*>(p)[i];
         t.l = lo ? lo[i] : (int8_t)0;

@@ -24,6 +24,7 @@ struct Runner {
     bool graph_failed = false;
     long long launches = 0;            // kernels issued (graph replays count their nodes)
     int* d_err = nullptr;              // set by a staged kernel whose bounded wait expired
+    size_t d_err_bytes = 0;            // its block (from the arena cache)
     int variant = BP_KERNEL_AUTO;      // BP_KERNEL_*: which phase-kernel family runs
 
     void configure(int prec_, int dim_, int order_, const ShotDesc* d, int n, long long tiles, long long tiles_s,
@@ -41,7 +42,9 @@ struct Runner {
         select_kernels();
         grid_s = (int)(sms < tiles_s ? sms : (tiles_s > 0 ? tiles_s : 1));
         if (!d_err) {
-            if (cudaMalloc(&d_err, sizeof(int)) == cudaSuccess) cudaMemsetAsync(d_err, 0, sizeof(int), st);
+            // from the arena cache: a cudaFree, even of 4 bytes, stalled the
+            // host for up to 0.6 s when the simulation was destroyed
+            if (arena_alloc(256, (void**)&d_err, &d_err_bytes) == cudaSuccess) cudaMemsetAsync(d_err, 0, sizeof(int), st);
             else d_err = nullptr;
         }
         graph_steps = steps_per_graph;
@@ -62,7 +65,7 @@ struct Runner {
     }
     ~Runner() {
         reset_graph();
-        if (d_err) cudaFree(d_err);
+        if (d_err) arena_release(d_err, d_err_bytes);
     }
 
     cudaError_t phase(bool v, int k) {

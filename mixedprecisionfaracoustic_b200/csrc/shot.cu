@@ -48,7 +48,13 @@ int validate_config(const bp_config* c) {
     const int hw = c->order / 2;
     const int nx = c->nx + 2 * c->npml, nz = c->nz + 2 * c->npml, ny = c->dim == 3 ? c->ny + 2 * c->npml : 1;
     if (nx < 2 * hw + 1 || nz < 2 * hw + 1 || (c->dim == 3 && ny < 2 * hw + 1)) { set_error("grid smaller than the stencil"); return BP_ERR_ARG; }
-    if ((long long)nx * ny * nz > (1LL << 40)) { set_error("grid too large"); return BP_ERR_ARG; }
+    // the phase kernels address cells with 32-bit offsets: every array (row
+    // pitch x ny x nz cells, the pitch rounded up to 32) holds < 2^31 elements
+    if ((long long)((nx + 31) & ~31) * ny * nz >= (1LL << 31)) {
+        set_error("grid too large: the padded grid (row pitch x ny x nz, pitch = nx + 2 npml rounded up to 32) "
+                  "must hold fewer than 2^31 cells");
+        return BP_ERR_ARG;
+    }
     if (!(c->dx > 0) || !(c->dt > 0) || c->nt < 1) { set_error("dx, dt must be > 0 and nt >= 1"); return BP_ERR_ARG; }
     if (!(c->f0 > 0)) { set_error("f0 must be > 0"); return BP_ERR_ARG; }
     if (c->npml > 0 && (!(c->pml_v0 > 0) || !(c->pml_r > 0) || !(c->pml_r < 1))) { set_error("bad CPML parameters"); return BP_ERR_ARG; }
@@ -476,12 +482,19 @@ size_t arena_cache_limit(int device) {
         env = v ? atoll(v) : -1;
     }
     if (env >= 0) return (size_t)env << 20;
+    // the device's total memory, queried once per device (cudaMemGetInfo took
+    // tens of ms in some calls, and this runs on every release)
+    static std::mutex mu;
+    static std::map<int, size_t> limits;
+    std::lock_guard<std::mutex> g(mu);
+    auto it = limits.find(device);
+    if (it != limits.end()) return it->second;
     size_t total = 0, freeb = 0;
     int cur = -1;
     cudaGetDevice(&cur);
     if (cur != device) return 0;
     if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) { cudaGetLastError(); return 0; }
-    return std::min(total / 4, (size_t)32 << 30);
+    return limits[device] = std::min(total / 4, (size_t)32 << 30);
 }
 
 void free_cached(int device) {   // g_arena_mu held; device -1 = all devices

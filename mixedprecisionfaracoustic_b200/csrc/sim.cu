@@ -60,10 +60,17 @@ static int check_device(int device) {
         return BP_ERR_NO_DEVICE;
     }
     if (device < 0 || device >= n) { set_error("device ordinal out of range"); return BP_ERR_ARG; }
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { set_error("cudaGetDeviceProperties failed"); return BP_ERR_NO_DEVICE; }
-    if (prop.major != 10) {
-        set_error("this library is built for sm_100a (B200); device is sm_" + std::to_string(prop.major) + std::to_string(prop.minor));
+    // two attribute queries: cudaGetDeviceProperties fills every field and took
+    // 5-60 ms per call, inside every bp_create
+    int major = 0, minor = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cannot query the device's compute capability");
+        return BP_ERR_NO_DEVICE;
+    }
+    if (major != 10) {
+        set_error("this library is built for sm_100a (B200); device is sm_" + std::to_string(major) + std::to_string(minor));
         return BP_ERR_NO_DEVICE;
     }
     return BP_OK;

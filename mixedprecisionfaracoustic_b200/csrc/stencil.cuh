@@ -52,7 +52,7 @@ __device__ __forceinline__ R rbwd(const R* a) {
 // Load f(x0 - HW .. x0 + 3 + HW) of one row; x neighbours clamped into the row
 // (clamped values only feed cells that are never updated).
 template <int ORD, class P>
-__device__ __forceinline__ void load_span(const void* p, const int8_t* lo, long long rowbase, int x0, int nx,
+__device__ __forceinline__ void load_span(const void* p, const int8_t* lo, cidx rowbase, int x0, int nx,
                                           typename P::real (&v)[4 + ORD]) {
     constexpr int HW = ORD / 2;
     typename P::real c[4];
@@ -70,11 +70,11 @@ __device__ __forceinline__ void load_span(const void* p, const int8_t* lo, long 
 
 // Load the 4 cells of rows row-HW .. row+HW (offsets along y or z).
 template <int ORD, class P>
-__device__ __forceinline__ void load_rows(const void* p, const int8_t* lo, long long c, long long stride,
+__device__ __forceinline__ void load_rows(const void* p, const int8_t* lo, cidx c, cidx stride,
                                           typename P::real (&a)[ORD + 1][4]) {
     constexpr int HW = ORD / 2;
 #pragma unroll
-    for (int k = 0; k <= ORD; k++) P::ld4(p, lo, c + (long long)(k - HW) * stride, a[k]);
+    for (int k = 0; k <= ORD; k++) P::ld4(p, lo, c + (k - HW) * stride, a[k]);
 }
 
 // Product by the COMP16 rescale factor, never fused into a neighbouring add:
@@ -158,7 +158,7 @@ struct PsiIO {
 // One derivative slot of one axis: memory variables k (ψ) and NS+k (prev) of
 // the (phase, axis) slab array; fwd selects the half-grid profile.
 template <int NS, bool RS, class R>
-__device__ __forceinline__ void cpml_slot(R (&d)[4], void* base, long long cells, int k, long long sidx,
+__device__ __forceinline__ void cpml_slot(R (&d)[4], void* base, long long cells, int k, cidx sidx,
                                           bool xaxis, int pos, int x0, const void* pb, const void* pe, R r) {
     R* ps = static_cast<R*>(base) + (long long)k * cells + sidx;
     R* pv = static_cast<R*>(base) + (long long)(NS + k) * cells + sidx;
@@ -174,20 +174,20 @@ __device__ __forceinline__ void cpml_slot(R (&d)[4], void* base, long long cells
 }
 
 // Slab memory-variable index of a chunk for one axis, or -1 outside the slab.
-__device__ __forceinline__ long long slab_index(const ShotDesc& S, int axis, int x0, int y, int z) {
+__device__ __forceinline__ cidx slab_index(const ShotDesc& S, int axis, int x0, int y, int z) {
     const Slab& sl = S.slab[axis];
     if (axis == 0) {
         int sx = sl.index(x0);
         if (sx < 0) return -1;
-        return ((long long)z * S.ny + y) * sl.width + sx;
+        return (z * S.ny + y) * sl.width + sx;
     } else if (axis == 1) {
         int sy = sl.index(y);
         if (sy < 0) return -1;
-        return ((long long)z * sl.width + sy) * S.pitch + x0;
+        return (z * sl.width + sy) * S.pitch + x0;
     } else {
         int sz = sl.index(z);
         if (sz < 0) return -1;
-        return ((long long)sz * S.ny + y) * S.pitch + x0;
+        return (sz * S.ny + y) * S.pitch + x0;
     }
 }
 
@@ -207,7 +207,7 @@ struct VState {
 };
 
 template <int DIM, int ORD, class P, bool PRE, bool RS>
-__device__ __forceinline__ void v_tail(const ShotDesc& S, long long c, int x0, int y, int z, typename P::real r,
+__device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y, int z, typename P::real r,
                                        unsigned mask, VState<typename P::real>& V) {
     using R = typename P::real;
     auto &x1 = V.x1, &x3 = V.x3, &s1 = V.s1, &z1 = V.z1, &z2 = V.z2, &s3 = V.s3;
@@ -239,7 +239,7 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, long long c, int x0, i
     // ---- CPML memory variables on the slabs (Float/main.cu:130-158) ----
     {
         constexpr int NS = DIM == 3 ? 4 : 3;
-        long long si = slab_index(S, 0, x0, y, z);
+        cidx si = slab_index(S, 0, x0, y, z);
         if (si >= 0) {
             void* B = S.psiV[0];
             const long long n = S.slab_cells[0];
@@ -340,7 +340,7 @@ struct TState {
 };
 
 template <int DIM, int ORD, class P, bool PRE, bool RS>
-__device__ __forceinline__ void t_tail(const ShotDesc& S, long long c, int x0, int y, int z, typename P::real r,
+__device__ __forceinline__ void t_tail(const ShotDesc& S, cidx c, int x0, int y, int z, typename P::real r,
                                        unsigned mask, TState<typename P::real>& T) {
     using R = typename P::real;
     auto &uxx = T.uxx, &uzz = T.uzz, &wx = T.wx, &wz = T.wz, &uxz = T.uxz, &uzx = T.uzx;
@@ -381,7 +381,7 @@ __device__ __forceinline__ void t_tail(const ShotDesc& S, long long c, int x0, i
     // stored ψ/prev of this phase are old state and take the rescale r ----
     {
         constexpr int NS = DIM == 3 ? 4 : 3;
-        long long si = slab_index(S, 0, x0, y, z);
+        cidx si = slab_index(S, 0, x0, y, z);
         if (si >= 0) {
             void* B = S.psiT[0];
             const long long n = S.slab_cells[0];

@@ -103,9 +103,9 @@ template <int DIM, int ORD, class P, bool RS>
 __device__ __forceinline__ void v_chunk(const ShotDesc& S, int x0, int y, int z, typename P::real r,
                                         unsigned mask) {
     using R = typename P::real;
-    const long long sy = S.pitch, sz = S.plane;
-    const long long c = x0 + (long long)y * sy + (long long)z * sz;
-    const long long row = c - x0;
+    const cidx sy = S.pitch, sz = S.plane;
+    const cidx c = x0 + y * sy + z * sz;
+    const cidx row = c - x0;
 
     VState<R> V;
     auto &x1 = V.x1, &x3 = V.x3, &s1 = V.s1, &z1 = V.z1, &z2 = V.z2, &s3 = V.s3;
@@ -187,9 +187,9 @@ template <int DIM, int ORD, class P, bool RS>
 __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z, typename P::real r,
                                         unsigned mask) {
     using R = typename P::real;
-    const long long sy = S.pitch, sz = S.plane;
-    const long long c = x0 + (long long)y * sy + (long long)z * sz;
-    const long long row = c - x0;
+    const cidx sy = S.pitch, sz = S.plane;
+    const cidx c = x0 + y * sy + z * sz;
+    const cidx row = c - x0;
 
     TState<R> T;
     auto &uxx = T.uxx, &uzz = T.uzz, &wx = T.wx, &wz = T.wz, &uxz = T.uxz, &uzx = T.uzx;
@@ -306,7 +306,7 @@ __host__ __device__ constexpr bool grouped() {
 
 // Difference along x of one field at the chunk (span load), divided by H.
 template <int ORD, class P, bool FWD>
-__device__ __forceinline__ void d_span(const ShotDesc& S, int f, long long row, int x0,
+__device__ __forceinline__ void d_span(const ShotDesc& S, int f, cidx row, int x0,
                                        typename P::real (&d)[4]) {
     typename P::real v[4 + ORD];
     load_span<ORD, P>(S.f[f], S.flo[f], row, x0, S.nx, v);
@@ -315,7 +315,7 @@ __device__ __forceinline__ void d_span(const ShotDesc& S, int f, long long row, 
 }
 // Difference across rows (y or z) of one field at the chunk, divided by H.
 template <int ORD, class P, bool FWD>
-__device__ __forceinline__ void d_rows(const ShotDesc& S, int f, long long c, long long stride,
+__device__ __forceinline__ void d_rows(const ShotDesc& S, int f, cidx c, cidx stride,
                                        typename P::real (&d)[4]) {
     using R = typename P::real;
     R a[ORD + 1][4];
@@ -339,7 +339,7 @@ __device__ __forceinline__ void mask0(R (&d)[4], unsigned mask) {
 // half); nothing outside that slab.  Slabs hold 3 slots per phase in 2D, 4 in 3D.
 template <int DIM, bool RS, class R>
 __device__ __forceinline__ void cpml_g(const ShotDesc& S, void* const (&psi)[3], int axis, int k, bool half,
-                                       long long si, int x0, int y, int z, R (&d)[4], R r) {
+                                       cidx si, int x0, int y, int z, R (&d)[4], R r) {
     if (si < 0) return;
     const void* pb = half ? S.pb2[axis] : S.pb[axis];
     const void* pe = half ? S.pe2[axis] : S.pe[axis];
@@ -350,10 +350,10 @@ __device__ __forceinline__ void cpml_g(const ShotDesc& S, void* const (&psi)[3],
 // One velocity component AX (0 = x, 1 = y, 2 = z) of the V phase
 // (Float/main.cu:103-191 for that component).
 template <int DIM, int ORD, class P, bool RS, int AX>
-__device__ __forceinline__ void v_comp(const ShotDesc& S, long long c, long long row, int x0, int y, int z,
+__device__ __forceinline__ void v_comp(const ShotDesc& S, cidx c, cidx row, int x0, int y, int z,
                                        typename P::real r, unsigned mask, const typename P::real (&rf)[4]) {
     using R = typename P::real;
-    const long long sy = S.pitch, sz = S.plane;
+    const cidx sy = S.pitch, sz = S.plane;
     // dx, dy, dz: the stress derivatives summed into this component (dy in 3D
     // only); dp: the pressure derivative along AX.  Slots as in v_tail.
     R dx[4], dy[4], dz[4], dp[4];
@@ -380,8 +380,8 @@ __device__ __forceinline__ void v_comp(const ShotDesc& S, long long c, long long
     mask0(dx, mask); mask0(dz, mask); mask0(dp, mask);
     if constexpr (DIM == 3) mask0(dy, mask);
     void* const psi[3] = {S.psiV[0], S.psiV[1], S.psiV[2]};
-    const long long s0 = slab_index(S, 0, x0, y, z), s2 = slab_index(S, 2, x0, y, z);
-    const long long s1 = DIM == 3 ? slab_index(S, 1, x0, y, z) : -1;
+    const cidx s0 = slab_index(S, 0, x0, y, z), s2 = slab_index(S, 2, x0, y, z);
+    const cidx s1 = DIM == 3 ? slab_index(S, 1, x0, y, z) : -1;
     if constexpr (AX == 0) {
         cpml_g<DIM, RS>(S, psi, 0, 0, true, s0, x0, y, z, dx, r);
         cpml_g<DIM, RS>(S, psi, 0, 1, true, s0, x0, y, z, dp, r);
@@ -443,8 +443,8 @@ template <int DIM, int ORD, class P, bool RS>
 __device__ __forceinline__ void v_chunk_g(const ShotDesc& S, int x0, int y, int z, typename P::real r,
                                           unsigned mask) {
     using R = typename P::real;
-    const long long c = x0 + (long long)y * S.pitch + (long long)z * S.plane;
-    const long long row = c - x0;
+    const cidx c = x0 + y * S.pitch + z * (cidx)S.plane;
+    const cidx row = c - x0;
     R rf[4];
     P::ld4(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, rf);
     v_comp<DIM, ORD, P, RS, 0>(S, c, row, x0, y, z, r, mask, rf);
@@ -454,13 +454,13 @@ __device__ __forceinline__ void v_chunk_g(const ShotDesc& S, int x0, int y, int 
 
 // Old value of a stress field at the chunk, with this step's rescale.
 template <class P, bool RS>
-__device__ __forceinline__ void ld_old(const ShotDesc& S, int f, long long c, typename P::real r,
+__device__ __forceinline__ void ld_old(const ShotDesc& S, int f, cidx c, typename P::real r,
                                        typename P::real (&o)[4]) {
     P::ld4(S.f[f], S.flo[f], c, o);
     if constexpr (P::prec == BP_PREC_COMP16 && RS) scale4(o, r);
 }
 template <class P>
-__device__ __forceinline__ void st_new(const ShotDesc& S, int f, long long c, unsigned mask,
+__device__ __forceinline__ void st_new(const ShotDesc& S, int f, cidx c, unsigned mask,
                                        typename P::real (&nv)[4], const typename P::real (&ov)[4]) {
 #pragma unroll
     for (int j = 0; j < 4; j++)
@@ -471,10 +471,10 @@ __device__ __forceinline__ void st_new(const ShotDesc& S, int f, long long c, un
 // One shear stress of the T phase: SH 0 = txy, 1 = tyz (3D only), 2 = txz
 // (Float/main.cu:232-294 for that stress).
 template <int DIM, int ORD, class P, bool RS, int SH>
-__device__ __forceinline__ void t_shear(const ShotDesc& S, long long c, long long row, int x0, int y, int z,
+__device__ __forceinline__ void t_shear(const ShotDesc& S, cidx c, cidx row, int x0, int y, int z,
                                         typename P::real r, unsigned mask, void* const (&psi)[3]) {
     using R = typename P::real;
-    const long long sy = S.pitch, sz = S.plane;
+    const cidx sy = S.pitch, sz = S.plane;
     R a[4], b[4];    // the two derivatives, in the order of the update's sum
     if constexpr (SH == 0) {
         d_rows<ORD, P, true>(S, BP_F_VUX, c, sy, a);        // uxy
@@ -515,9 +515,9 @@ template <int DIM, int ORD, class P, bool RS>
 __device__ __forceinline__ void t_chunk_g(const ShotDesc& S, int x0, int y, int z, typename P::real r,
                                           unsigned mask) {
     using R = typename P::real;
-    const long long sy = S.pitch, sz = S.plane;
-    const long long c = x0 + (long long)y * sy + (long long)z * sz;
-    const long long row = c - x0;
+    const cidx sy = S.pitch, sz = S.plane;
+    const cidx c = x0 + y * sy + z * sz;
+    const cidx row = c - x0;
     void* const psi[3] = {S.psiT[0], S.psiT[1], S.psiT[2]};
     if constexpr (DIM == 3) {
         t_shear<DIM, ORD, P, RS, 0>(S, c, row, x0, y, z, r, mask, psi);
@@ -538,15 +538,15 @@ __device__ __forceinline__ void t_chunk_g(const ShotDesc& S, int x0, int y, int 
     mask0(uxx, mask); mask0(wx, mask); mask0(uzz, mask); mask0(wz, mask);
     if constexpr (DIM == 3) { mask0(uyy, mask); mask0(wy, mask); }
     {
-        const long long s0 = slab_index(S, 0, x0, y, z);
+        const cidx s0 = slab_index(S, 0, x0, y, z);
         cpml_g<DIM, RS>(S, psi, 0, 0, false, s0, x0, y, z, uxx, r);
         cpml_g<DIM, RS>(S, psi, 0, 1, false, s0, x0, y, z, wx, r);
         if constexpr (DIM == 3) {
-            const long long s1 = slab_index(S, 1, x0, y, z);
+            const cidx s1 = slab_index(S, 1, x0, y, z);
             cpml_g<DIM, RS>(S, psi, 1, 0, false, s1, x0, y, z, uyy, r);
             cpml_g<DIM, RS>(S, psi, 1, 1, false, s1, x0, y, z, wy, r);
         }
-        const long long s2 = slab_index(S, 2, x0, y, z);
+        const cidx s2 = slab_index(S, 2, x0, y, z);
         cpml_g<DIM, RS>(S, psi, 2, 0, false, s2, x0, y, z, uzz, r);
         cpml_g<DIM, RS>(S, psi, 2, 1, false, s2, x0, y, z, wz, r);
     }

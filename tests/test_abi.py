@@ -55,6 +55,24 @@ def test_create_rejects_bad_config(bad):
     assert rc == _abi.BP_ERR_ARG
 
 
+def test_create_rejects_grids_of_2_31_cells():
+    """Arrays are addressed with 32-bit cell offsets: a padded grid (row pitch x
+    ny x nz) of 2^31 cells or more is refused before any device work; one just
+    below the limit passes the check (and, without a GPU, fails at the device
+    check that follows)."""
+    cfg, med = config0(n=16, npml=4, nt=10, nrec=8)
+    lib = _abi.load()
+    # pitch 2048 (nx + 2 npml = 2048), ny = 1024, nz = 1024: exactly 2^31 cells
+    cfg.nx, cfg.ny, cfg.nz, cfg.npml = 2040, 1016, 1016, 4
+    rc, _ = _create(cfg, med)
+    assert rc == _abi.BP_ERR_ARG
+    assert b"2^31" in lib.bp_last_error()
+    if not has_gpu():                               # the medium here is far smaller than that grid
+        cfg.nz = 1015                               # 2^31 - 2^21 cells
+        rc, _ = _create(cfg, med)
+        assert rc == _abi.BP_ERR_NO_DEVICE
+
+
 def test_create_without_gpu_fails_loudly():
     if has_gpu():
         pytest.skip("a GPU is present")
