@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "runner.h"
@@ -103,23 +104,37 @@ int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out) {
     if (rc) return rc;
     rc = check_device(cfg->device);
     if (rc) return rc;
-    if (cfg->check_cfl && medium) {
-        double dtmax = 0, vmax = 0;
-        rc = bp_cfl_limit(cfg, medium, &dtmax, &vmax);
-        if (rc) return rc;
+    // The stability check scans the host medium on host threads while this
+    // thread sets up the device (medium upload, precompute kernels); both only
+    // read the medium.  A failing check undoes the set-up.
+    double dtmax = 0, vmax = 0;
+    int cfl_rc = BP_OK;
+    std::thread cfl;
+    if (cfg->check_cfl && medium)
+        cfl = std::thread([&] { cfl_rc = bp_cfl_limit(cfg, medium, &dtmax, &vmax); });
+    // joins the scan; reports its failure unless an earlier one is being returned
+    auto cfl_verdict = [&](bool report) -> int {
+        if (!cfl.joinable()) return BP_OK;
+        cfl.join();
+        if (!report) return BP_OK;
+        if (cfl_rc) { set_error("stability check: bad medium arrays"); return cfl_rc; }
         if ((double)cfg->dt > dtmax) {
             char buf[160];
             snprintf(buf, sizeof buf, "dt=%g exceeds the stability limit %g (vmax=%g m/s)", (double)cfg->dt, dtmax, vmax);
             set_error(buf);
             return BP_ERR_CFL;
         }
-    }
-    SIM_CK(cudaSetDevice(cfg->device));
+        return BP_OK;
+    };
+    cudaError_t e = cudaSetDevice(cfg->device);
+    if (e != cudaSuccess) { cfl_verdict(false); set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
     bp_sim* s = new bp_sim();
     s->device = cfg->device;
-    cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
-    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); delete s; return BP_ERR_CUDA; }
+    e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { cfl_verdict(false); set_error(cudaGetErrorString(e)); delete s; return BP_ERR_CUDA; }
     rc = s->shot.create(cfg, medium, s->st);
+    const int crc = cfl_verdict(rc == BP_OK);
+    if (!rc && crc) { cudaStreamSynchronize(s->st); rc = crc; }
     if (rc) { s->shot.destroy(); cudaStreamDestroy(s->st); delete s; return rc; }
     s->run.configure(cfg->precision, cfg->dim, cfg->order, s->shot.d_desc, 1, s->shot.ntiles, s->shot.ntiles_s,
                      s->shot.ntiles_m, s->shot.nurec, s->st, 0, 32);

@@ -74,3 +74,21 @@ def test_server_fails_the_unstable_request_only():
     st = srv.stats()
     assert st["failed"] == 1 and st["completed"] == 1
     srv.close()
+
+
+def test_create_refuses_a_time_step_above_the_stability_limit():
+    """With the check on, bp_create refuses dt above the limit (the check runs
+    beside the device set-up, which is then undone), and a healthy shot created
+    right after runs as usual."""
+    cfg, med = unstable()
+    cfg.check_cfl = 1
+    with pytest.raises(BiotError) as e:
+        Simulation(cfg, med)
+    assert e.value.code == _abi.BP_ERR_CFL
+    assert "stability limit" in str(e.value)
+    cfg, med = healthy()
+    cfg.check_cfl = 1
+    with Simulation(cfg, med) as s:
+        s.run(cfg.nt)
+        s.sync()
+        assert np.isfinite(s.traces("txx")).all() and np.abs(s.traces("txx")).max() > 0
