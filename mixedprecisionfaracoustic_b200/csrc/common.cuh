@@ -144,17 +144,34 @@ __device__ __forceinline__ void encode_ch(float v, __half& hi, int8_t& lo) {
     lo = (int8_t)q;
 }
 
+// Loads of arrays that no thread writes while the kernel runs (the fields a
+// phase differentiates and the coefficients) may take the read-only data path
+// (__ldg).  Measured on B200, bit-identical either way: the 2D FP32 T phase
+// 2.7 % faster, the 3D order-4 FP32 V phase 4 % slower, COMP16 and the large 3D
+// grid unchanged; so off by default.
+#ifndef BP_NC_LOADS
+#define BP_NC_LOADS 0
+#endif
+constexpr bool kReadOnlyPath = BP_NC_LOADS;
+template <bool NC, class T>
+__device__ __forceinline__ T ldv(const T* p) {
+    if constexpr (NC) return __ldg(p);
+    else return *p;
+}
+
 // ---------------------------------------------------------------------------
 // Precision policies: storage of fields/coefficients and the arithmetic type.
 struct PolF32 {
     using real = float;
     static constexpr int prec = BP_PREC_FP32;
+    template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
-        float4 t = *reinterpret_cast<const float4*>(static_cast<const float*>(p) + i);
+        float4 t = ldv<NC>(reinterpret_cast<const float4*>(static_cast<const float*>(p) + i));
         v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
     }
+    template <bool NC = false>
     __device__ __forceinline__ static real ld1(const void* p, const int8_t*, cidx i) {
-        return static_cast<const float*>(p)[i];
+        return ldv<NC>(static_cast<const float*>(p) + i);
     }
     __device__ __forceinline__ static void st4(void* p, int8_t*, cidx i, const real (&v)[4]) {
         *reinterpret_cast<float4*>(static_cast<float*>(p) + i) = make_float4(v[0], v[1], v[2], v[3]);
@@ -182,13 +199,15 @@ struct PolF32 {
 struct PolF64 {
     using real = double;
     static constexpr int prec = BP_PREC_FP64;
+    template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
         const double2* q = reinterpret_cast<const double2*>(static_cast<const double*>(p) + i);
-        double2 a = q[0], b = q[1];
+        double2 a = ldv<NC>(q), b = ldv<NC>(q + 1);
         v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
     }
+    template <bool NC = false>
     __device__ __forceinline__ static real ld1(const void* p, const int8_t*, cidx i) {
-        return static_cast<const double*>(p)[i];
+        return ldv<NC>(static_cast<const double*>(p) + i);
     }
     __device__ __forceinline__ static void st4(void* p, int8_t*, cidx i, const real (&v)[4]) {
         double2* q = reinterpret_cast<double2*>(static_cast<double*>(p) + i);
@@ -220,13 +239,14 @@ struct PolF64 {
 struct PolC16 {
     using real = float;
     static constexpr int prec = BP_PREC_COMP16;
+    template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t* lo, cidx i, real (&v)[4]) {
-        uint2 h = *reinterpret_cast<const uint2*>(static_cast<const __half*>(p) + i);
+        uint2 h = ldv<NC>(reinterpret_cast<const uint2*>(static_cast<const __half*>(p) + i));
         __half2 h01 = *reinterpret_cast<__half2*>(&h.x);
         __half2 h23 = *reinterpret_cast<__half2*>(&h.y);
         __half hs[4] = {__low2half(h01), __high2half(h01), __low2half(h23), __high2half(h23)};
         if (lo) {
-            char4 l = *reinterpret_cast<const char4*>(lo + i);
+            char4 l = ldv<NC>(reinterpret_cast<const char4*>(lo + i));
             v[0] = decode_ch(hs[0], l.x); v[1] = decode_ch(hs[1], l.y);
             v[2] = decode_ch(hs[2], l.z); v[3] = decode_ch(hs[3], l.w);
         } else {
@@ -234,9 +254,10 @@ struct PolC16 {
             for (int j = 0; j < 4; j++) v[j] = __half2float(hs[j]);
         }
     }
+    template <bool NC = false>
     __device__ __forceinline__ static real ld1(const void* p, const int8_t* lo, cidx i) {
-        __half h = static_cast<const __half*>(p)[i];
-        return lo ? decode_ch(h, lo[i]) : __half2float(h);
+        __half h = ldv<NC>(static_cast<const __half*>(p) + i);
+        return lo ? decode_ch(h, ldv<NC>(reinterpret_cast<const signed char*>(lo) + i)) : __half2float(h);
     }
     __device__ __forceinline__ static void st4(void* p, int8_t* lo, cidx i, const real (&v)[4]) {
         __half hs[4];
