@@ -51,30 +51,30 @@ __device__ __forceinline__ R rbwd(const R* a) {
 
 // Load f(x0 - HW .. x0 + 3 + HW) of one row; x neighbours clamped into the row
 // (clamped values only feed cells that are never updated).
-template <int ORD, class P>
+template <int ORD, class P, bool NC = kReadOnlyPath>
 __device__ __forceinline__ void load_span(const void* p, const int8_t* lo, cidx rowbase, int x0, int nx,
                                           typename P::real (&v)[4 + ORD]) {
     constexpr int HW = ORD / 2;
     typename P::real c[4];
-    P::template ld4<kReadOnlyPath>(p, lo, rowbase + x0, c);
+    P::template ld4<NC>(p, lo, rowbase + x0, c);
 #pragma unroll
     for (int j = 0; j < 4; j++) v[HW + j] = c[j];
 #pragma unroll
     for (int k = 1; k <= HW; k++) {
         int xl = x0 - k; xl = xl < 0 ? 0 : xl;
         int xr = x0 + 3 + k; xr = xr > nx - 1 ? nx - 1 : xr;
-        v[HW - k] = P::template ld1<kReadOnlyPath>(p, lo, rowbase + xl);
-        v[HW + 3 + k] = P::template ld1<kReadOnlyPath>(p, lo, rowbase + xr);
+        v[HW - k] = P::template ld1<NC>(p, lo, rowbase + xl);
+        v[HW + 3 + k] = P::template ld1<NC>(p, lo, rowbase + xr);
     }
 }
 
 // Load the 4 cells of rows row-HW .. row+HW (offsets along y or z).
-template <int ORD, class P>
+template <int ORD, class P, bool NC = kReadOnlyPath>
 __device__ __forceinline__ void load_rows(const void* p, const int8_t* lo, cidx c, cidx stride,
                                           typename P::real (&a)[ORD + 1][4]) {
     constexpr int HW = ORD / 2;
 #pragma unroll
-    for (int k = 0; k <= ORD; k++) P::template ld4<kReadOnlyPath>(p, lo, c + (k - HW) * stride, a[k]);
+    for (int k = 0; k <= ORD; k++) P::template ld4<NC>(p, lo, c + (k - HW) * stride, a[k]);
 }
 
 // Product by the COMP16 rescale factor, never fused into a neighbouring add:
@@ -206,7 +206,7 @@ struct VState {
     R rho_y[4], c1_y[4], c2_y[4], vu_y[4], vw_y[4];
 };
 
-template <int DIM, int ORD, class P, bool PRE, bool RS>
+template <int DIM, int ORD, class P, bool PRE, bool RS, bool NC = kReadOnlyPath>
 __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y, int z, typename P::real r,
                                        unsigned mask, VState<typename P::real>& V) {
     using R = typename P::real;
@@ -217,9 +217,9 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y,
     auto &rho_y = V.rho_y, &c1_y = V.c1_y, &c2_y = V.c2_y, &vu_y = V.vu_y, &vw_y = V.vw_y;
     auto load_axis = [&](int fu, int fw, int crho, int ccc1, int ccc2, R (&rho)[4], R (&c1)[4], R (&c2)[4],
                          R (&vu)[4], R (&vw)[4]) {
-        P::template ld4<kReadOnlyPath>(S.vc[crho], S.vclo[crho], c, rho);
-        P::template ld4<kReadOnlyPath>(S.vc[ccc1], S.vclo[ccc1], c, c1);
-        P::template ld4<kReadOnlyPath>(S.vc[ccc2], S.vclo[ccc2], c, c2);
+        P::template ld4<NC>(S.vc[crho], S.vclo[crho], c, rho);
+        P::template ld4<NC>(S.vc[ccc1], S.vclo[ccc1], c, c1);
+        P::template ld4<NC>(S.vc[ccc2], S.vclo[ccc2], c, c2);
         P::ld4(S.f[fu], S.flo[fu], c, vu);
         P::ld4(S.f[fw], S.flo[fw], c, vw);
     };
@@ -314,7 +314,7 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y,
         P::st4(S.f[fu], S.flo[fu], c, nu);
     };
     if constexpr (!PRE) {
-        P::template ld4<kReadOnlyPath>(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, rf);
+        P::template ld4<NC>(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, rf);
         load_axis(BP_F_VUX, BP_F_VWX, VC_RHO_X, VC_CC1_X, VC_CC2_X, rho_x, c1_x, c2_x, vu_x, vw_x);
     }
     axis_update(sumx, s1, BP_F_VUX, BP_F_VWX, rho_x, c1_x, c2_x, vu_x, vw_x);
@@ -339,7 +339,7 @@ struct TState {
     R mxy[4], myz[4], oyy[4], oxy[4], oyz[4];
 };
 
-template <int DIM, int ORD, class P, bool PRE, bool RS>
+template <int DIM, int ORD, class P, bool PRE, bool RS, bool NC = kReadOnlyPath>
 __device__ __forceinline__ void t_tail(const ShotDesc& S, cidx c, int x0, int y, int z, typename P::real r,
                                        unsigned mask, TState<typename P::real>& T) {
     using R = typename P::real;
@@ -349,18 +349,18 @@ __device__ __forceinline__ void t_tail(const ShotDesc& S, cidx c, int x0, int y,
     auto &op = T.op, &oxx = T.oxx, &ozz = T.ozz, &oxz = T.oxz;
     auto &mxy = T.mxy, &myz = T.myz, &oyy = T.oyy, &oxy = T.oxy, &oyz = T.oyz;
     auto load_state = [&]() {
-        P::template ld4<kReadOnlyPath>(S.tc[TC_C], S.tclo[TC_C], c, cC);
-        P::template ld4<kReadOnlyPath>(S.tc[TC_M], S.tclo[TC_M], c, cM);
-        P::template ld4<kReadOnlyPath>(S.tc[TC_H], S.tclo[TC_H], c, cH);
-        P::template ld4<kReadOnlyPath>(S.tc[TC_H2U], S.tclo[TC_H2U], c, cH2);
-        P::template ld4<kReadOnlyPath>(S.tc[TC_MUXZ], S.tclo[TC_MUXZ], c, mxz);
+        P::template ld4<NC>(S.tc[TC_C], S.tclo[TC_C], c, cC);
+        P::template ld4<NC>(S.tc[TC_M], S.tclo[TC_M], c, cM);
+        P::template ld4<NC>(S.tc[TC_H], S.tclo[TC_H], c, cH);
+        P::template ld4<NC>(S.tc[TC_H2U], S.tclo[TC_H2U], c, cH2);
+        P::template ld4<NC>(S.tc[TC_MUXZ], S.tclo[TC_MUXZ], c, mxz);
         P::ld4(S.f[BP_F_P], S.flo[BP_F_P], c, op);
         P::ld4(S.f[BP_F_TXX], S.flo[BP_F_TXX], c, oxx);
         P::ld4(S.f[BP_F_TZZ], S.flo[BP_F_TZZ], c, ozz);
         P::ld4(S.f[BP_F_TXZ], S.flo[BP_F_TXZ], c, oxz);
         if constexpr (DIM == 3) {
-            P::template ld4<kReadOnlyPath>(S.tc[TC_MUXY], S.tclo[TC_MUXY], c, mxy);
-            P::template ld4<kReadOnlyPath>(S.tc[TC_MUYZ], S.tclo[TC_MUYZ], c, myz);
+            P::template ld4<NC>(S.tc[TC_MUXY], S.tclo[TC_MUXY], c, mxy);
+            P::template ld4<NC>(S.tc[TC_MUYZ], S.tclo[TC_MUYZ], c, myz);
             P::ld4(S.f[BP_F_TYY], S.flo[BP_F_TYY], c, oyy);
             P::ld4(S.f[BP_F_TXY], S.flo[BP_F_TXY], c, oxy);
             P::ld4(S.f[BP_F_TYZ], S.flo[BP_F_TYZ], c, oyz);
