@@ -64,6 +64,8 @@ int BatchCore::rebuild() {
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);   // h is a local buffer
         if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
     }
+    run.post_in_t = true;
+    for (auto& sh : shots) run.post_in_t = run.post_in_t && sh->post_in_t;
     run.configure(prec, dim, order, d_descs, n, t0, t0s, t0m, maxrec, st, ctas_per_sm,
                   steps_per_sync > 0 ? steps_per_sync : 32);
     return BP_OK;

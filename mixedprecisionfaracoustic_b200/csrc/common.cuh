@@ -101,6 +101,11 @@ struct ShotDesc {
     long long tile0m;             // first task of this shot in the marching tiling
     int zseg_m;                   // rows per marching task
     int pad_m;
+    // receivers by row, for the T phase that records them itself: the unique
+    // receivers of row key (3D: z * ny + y, 2D: z) are rec_xu[rec_row[key] ..
+    // rec_row[key + 1]), sorted by x, each as (x, unique receiver index)
+    const int* rec_row;
+    const int2* rec_xu;
     template <class R>
     __device__ __forceinline__ R dtr() const { return sizeof(R) == 8 ? (R)dtd : (R)dt; }
 };

@@ -26,6 +26,7 @@ struct Runner {
     int* d_err = nullptr;              // set by a staged kernel whose bounded wait expired
     size_t d_err_bytes = 0;            // its block (from the arena cache)
     int variant = BP_KERNEL_AUTO;      // BP_KERNEL_*: which phase-kernel family runs
+    bool post_in_t = false;            // every shot's receivers and source lie in cells the T phase visits
 
     void configure(int prec_, int dim_, int order_, const ShotDesc* d, int n, long long tiles, long long tiles_s,
                    long long tiles_m, int maxrec, cudaStream_t s, int ctas_per_sm, int steps_per_graph) {
@@ -68,10 +69,21 @@ struct Runner {
         if (d_err) arena_release(d_err, d_err_bytes);
     }
 
+    // The register kernels' T phase records the receivers and injects the
+    // next source sample itself where every shot allows it (one launch per
+    // step fewer); otherwise, and for the other kernel families, k_post does.
+    bool fused_post() const {
+#ifdef BP_POST_IN_T
+        if (!BP_POST_IN_T) return false;
+#endif
+        return post_in_t && !march && !staged;
+    }
+    int launches_per_step() const { return fused_post() ? 2 : 3; }
     cudaError_t phase(bool v, int k) {
         if (march) return launch_phase_march(prec, order, v, d_shots, nshots, ntiles_m, k, st);
         if (staged) return launch_phase_staged(prec, order, v, d_shots, nshots, ntiles_s, k, grid_s, d_err, st);
-        return launch_phase(prec, dim, order, v, d_shots, nshots, ntiles, k, v ? grid_v : grid_t, st);
+        return launch_phase(prec, dim, order, v, d_shots, nshots, ntiles, k, v ? grid_v : grid_t, st,
+                            (!v && fused_post()) ? 1 : 0);
     }
 
     // m steps issued directly (k = 0..m-1), then the step bases advance by m.
@@ -80,10 +92,10 @@ struct Runner {
         for (int k = 0; k < m && e == cudaSuccess; k++) {
             e = phase(true, k);
             if (e == cudaSuccess) e = phase(false, k);
-            if (e == cudaSuccess) e = launch_post(prec, d_shots, nshots, max_rec, k, 1, st);
+            if (e == cudaSuccess && !fused_post()) e = launch_post(prec, d_shots, nshots, max_rec, k, 1, st);
         }
         if (e == cudaSuccess) e = launch_advance(d_shots, nshots, m, st);
-        if (count) launches += 3LL * m + 1;
+        if (count) launches += (long long)launches_per_step() * m + 1;
         return e;
     }
     cudaError_t ensure_graph() {
@@ -104,7 +116,7 @@ struct Runner {
             ensure_graph();
             while (exec && m >= graph_steps && e == cudaSuccess) {
                 e = cudaGraphLaunch(exec, st);
-                launches += 3LL * graph_steps + 1;
+                launches += (long long)launches_per_step() * graph_steps + 1;
                 m -= graph_steps;
             }
         }

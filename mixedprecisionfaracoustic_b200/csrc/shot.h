@@ -12,8 +12,10 @@
 namespace bpk {
 
 // launchers (step.cu, precompute.cu, reduce.cu)
+// post = 1: the T phase also records the receivers and injects the next source
+// sample (every receiver and the source lie in cells the T phase visits)
 cudaError_t launch_phase(int prec, int dim, int order, bool vphase, const ShotDesc* d_shots, int nshots,
-                         long long ntiles, int k, int grid, cudaStream_t st);
+                         long long ntiles, int k, int grid, cudaStream_t st, int post = 0);
 cudaError_t launch_post(int prec, const ShotDesc* d_shots, int nshots, int max_rec, int k, int do_record,
                         cudaStream_t st);
 cudaError_t launch_inject(int prec, const ShotDesc* d_shots, int nshots, int k, cudaStream_t st);
@@ -86,6 +88,7 @@ struct Shot {
     long long ntiles = 0;              // tiles of the register kernels (128 x 8)
     long long ntiles_s = 0;            // tiles of the TMA-staged 2D kernels (256 x staged_tile_rows)
     long long ntiles_m = 0;            // tasks of the marching 2D kernels (128 cells x zseg_m rows)
+    bool post_in_t = false;            // receivers and source all in cells the T phase visits
 
     // The device regions that make up the shot's evolving state, in a fixed
     // order: wavefields (and COMP16 residuals), CPML memory variables of both

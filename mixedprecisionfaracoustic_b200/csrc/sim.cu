@@ -136,6 +136,7 @@ int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out) {
     const int crc = cfl_verdict(rc == BP_OK);
     if (!rc && crc) { cudaStreamSynchronize(s->st); rc = crc; }
     if (rc) { s->shot.destroy(); cudaStreamDestroy(s->st); delete s; return rc; }
+    s->run.post_in_t = s->shot.post_in_t;
     s->run.configure(cfg->precision, cfg->dim, cfg->order, s->shot.d_desc, 1, s->shot.ntiles, s->shot.ntiles_s,
                      s->shot.ntiles_m, s->shot.nurec, s->st, 0, 32);
     *out = s;
@@ -453,7 +454,7 @@ int bp_profile_phases(bp_sim* s, int nsteps, float ms[3]) {
         cudaEventRecord(ev[1], s->st);
         if (e == cudaSuccess) e = R.phase(false, 0);
         cudaEventRecord(ev[2], s->st);
-        if (e == cudaSuccess) e = launch_post(R.prec, R.d_shots, R.nshots, R.max_rec, 0, 1, s->st);
+        if (e == cudaSuccess && !R.fused_post()) e = launch_post(R.prec, R.d_shots, R.nshots, R.max_rec, 0, 1, s->st);
         if (e == cudaSuccess) e = launch_advance(R.d_shots, R.nshots, 1, s->st);
         cudaEventRecord(ev[3], s->st);
         if (e == cudaSuccess) e = cudaEventSynchronize(ev[3]);
@@ -462,7 +463,7 @@ int bp_profile_phases(bp_sim* s, int nsteps, float ms[3]) {
             cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
             acc[q] += t;
         }
-        R.launches += 4;
+        R.launches += R.launches_per_step() + 1;
     }
     for (auto& x : ev) cudaEventDestroy(x);
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }

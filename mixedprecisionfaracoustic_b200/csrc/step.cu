@@ -635,9 +635,15 @@ __device__ __forceinline__ void t_chunk_g(const ShotDesc& S, int x0, int y, int 
 
 // ---------------------------------------------------------------------------
 // Tile loop shared by both phases.
+template <int DIM, class P>
+__device__ __forceinline__ void post_chunk(const ShotDesc& S, int it, cidx c, int x0, int y, int z);
+
+// post (T phase only): each chunk also records the receivers in its cells and,
+// if it holds the source cell, injects the next source sample, in place of the
+// post-step kernel k_post.
 template <int DIM, int ORD, class P, bool VPHASE>
 __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHASE>())) k_phase(const ShotDesc* __restrict__ shots, int nshots,
-                                                     long long ntiles, int k) {
+                                                     long long ntiles, int k, int post) {
     using R = typename P::real;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // The descriptor of the tile's shot is staged in shared memory whenever the
@@ -646,6 +652,7 @@ __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHAS
     __shared__ ShotDesc sdesc;
     int cur = -1;
     bool live = false;
+    int it_cur = 0;
     R r = (R)1;
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int si = nshots == 1 ? 0 : locate_shot(shots, nshots, t);
@@ -660,6 +667,7 @@ __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHAS
                 // the step index and the COMP16 rescale are fixed for the
                 // whole launch: read them once per shot, not once per tile
                 const int it = *sdesc.step_base + k;
+                it_cur = it;
                 live = !sdesc.done && it < sdesc.nt;
                 if constexpr (P::prec == BP_PREC_COMP16) r = live ? sdesc.rtab[it] : 1.0f;
             }
@@ -675,6 +683,7 @@ __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHAS
         } else {
             const int it = *S.step_base + k;
             if (S.done || it >= S.nt) continue;
+            it_cur = it;
             if constexpr (P::prec == BP_PREC_COMP16) r = S.rtab[it];
             const long long lt = t - S.tile0;
             seg = (int)(lt % S.nseg);
@@ -720,6 +729,8 @@ __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHAS
             if constexpr (VPHASE) v_chunk<DIM, ORD, P, false>(S, x0, y, z, r, mask);
             else t_chunk<DIM, ORD, P, false>(S, x0, y, z, r, mask);
         }
+        if constexpr (!VPHASE)
+            if (post) post_chunk<DIM, P>(S, it_cur, x0 + y * (cidx)S.pitch + z * (cidx)S.plane, x0, y, z);
     }
 }
 
@@ -754,41 +765,78 @@ __device__ __forceinline__ void inject(const ShotDesc& S, int it) {
     if (S.src_mask & BP_SRC_P) P::st1(S.f[BP_F_P], S.flo[BP_F_P], i, P::ld1(S.f[BP_F_P], S.flo[BP_F_P], i) - I);
 }
 
+// Records step it's five components at unique receiver r, cell i.
+template <class P>
+__device__ __forceinline__ void record(const ShotDesc& S, int it, int r, long long i) {
+    using R = typename P::real;
+    R ss = (R)1, sv = (R)1;
+    if constexpr (P::prec == BP_PREC_COMP16) {
+        const float d = 1.0f / S.dyn[it];
+        ss = S.out_stress * d;
+        sv = S.out_vel * d;
+    }
+    R v[BP_NTRACE];
+    v[BP_TR_TXX] = read_phys<P>(S, BP_F_TXX, i, ss);
+    v[BP_TR_TZZ] = read_phys<P>(S, BP_F_TZZ, i, ss);
+    v[BP_TR_VUX] = read_phys<P>(S, BP_F_VUX, i, sv);
+    v[BP_TR_VWX] = read_phys<P>(S, BP_F_VWX, i, sv);
+    v[BP_TR_P] = read_phys<P>(S, BP_F_P, i, ss);
+    const long long cs = (long long)S.nrec * S.nt;
+    bool finite = true;
+#pragma unroll
+    for (int q = 0; q < BP_NTRACE; q++) {
+        S.traces[q * cs + (long long)r * S.nt + it] = (float)v[q];
+        if constexpr (P::prec == BP_PREC_FP64) S.traces64[q * cs + (long long)r * S.nt + it] = v[q];
+        finite = finite && isfinite(v[q]);
+    }
+    // blow-up detection: the first step whose recorded values are not all
+    // finite (step + 1; 0 = none), read by the host at its next sync
+    if (!finite) atomicCAS(S.blowup, 0, it + 1);
+}
+
 template <class P>
 __global__ void k_post(const ShotDesc* __restrict__ shots, int k, int do_record) {
-    using R = typename P::real;
     const ShotDesc& S = shots[blockIdx.y];
     const int it = *S.step_base + k;
     if (S.done || it >= S.nt) return;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (do_record && r < S.nrec && it < S.nt) {
-        const long long i = S.rec_idx[r];
-        R ss = (R)1, sv = (R)1;
-        if constexpr (P::prec == BP_PREC_COMP16) {
-            const float d = 1.0f / S.dyn[it];
-            ss = S.out_stress * d;
-            sv = S.out_vel * d;
-        }
-        R v[BP_NTRACE];
-        v[BP_TR_TXX] = read_phys<P>(S, BP_F_TXX, i, ss);
-        v[BP_TR_TZZ] = read_phys<P>(S, BP_F_TZZ, i, ss);
-        v[BP_TR_VUX] = read_phys<P>(S, BP_F_VUX, i, sv);
-        v[BP_TR_VWX] = read_phys<P>(S, BP_F_VWX, i, sv);
-        v[BP_TR_P] = read_phys<P>(S, BP_F_P, i, ss);
-        const long long cs = (long long)S.nrec * S.nt;
-        bool finite = true;
-#pragma unroll
-        for (int q = 0; q < BP_NTRACE; q++) {
-            S.traces[q * cs + (long long)r * S.nt + it] = (float)v[q];
-            if constexpr (P::prec == BP_PREC_FP64) S.traces64[q * cs + (long long)r * S.nt + it] = v[q];
-            finite = finite && isfinite(v[q]);
-        }
-        // blow-up detection: the first step whose recorded values are not all
-        // finite (step + 1; 0 = none), read by the host at its next sync
-        if (!finite) atomicCAS(S.blowup, 0, it + 1);
-    }
+    if (do_record && r < S.nrec) record<P>(S, it, r, S.rec_idx[r]);
     const bool owner = (S.src_rec >= 0) ? (r == S.src_rec) : (blockIdx.x == 0 && threadIdx.x == 0);
     if (owner) inject<P>(S, it + 1);
+}
+
+// k_post's work for the cells of one T-phase chunk (c = flat index of cell
+// x0), after the chunk's stores: the chunk's receivers, found by a binary
+// search of its row's x-sorted list, read back the values this thread has just
+// written (the velocities are not written in the T phase), so the recorded
+// values are k_post's; then the source, if its cell is here.  The receiver on
+// the source cell, if any, is recorded before the injection, as in k_post.
+// The recording and injection, out of line: only the few chunks that hold a
+// receiver or the source call it, and the phase kernels keep their registers.
+template <class P>
+__device__ __noinline__ void post_cells(const ShotDesc& S, int it, cidx c, int x0, int lo, int end) {
+    if (lo < end) {
+        int hi = end;
+        while (lo < hi) {                       // first receiver with x >= x0
+            const int mid = (lo + hi) >> 1;
+            if (S.rec_xu[mid].x < x0) lo = mid + 1;
+            else hi = mid;
+        }
+        for (; lo < end; lo++) {
+            const int2 xu = S.rec_xu[lo];
+            if (xu.x >= x0 + 4) break;
+            record<P>(S, it, xu.y, (long long)c + (xu.x - x0));
+        }
+    }
+    if (S.src_idx_valid && S.src_idx >= c && S.src_idx < (long long)c + 4) inject<P>(S, it + 1);
+}
+
+template <int DIM, class P>
+__device__ __forceinline__ void post_chunk(const ShotDesc& S, int it, cidx c, int x0, int y, int z) {
+    const int key = DIM == 3 ? z * S.ny + y : z;
+    const int lo = S.rec_row[key], end = S.rec_row[key + 1];
+    const bool src = S.src_idx_valid && S.src_idx >= c && S.src_idx < (long long)c + 4;
+    if (lo < end || src) post_cells<P>(S, it, c, x0, lo, end);
 }
 
 // Injection of step it = *step_base + k alone (before the first step).
@@ -874,11 +922,11 @@ __global__ void k_coef(const ShotDesc* __restrict__ shots, int which, float* out
 template <class P>
 struct Launch {
     static cudaError_t phase(int dim, int order, bool v, const ShotDesc* d_shots, int nshots, long long ntiles,
-                             int k, int grid, cudaStream_t st) {
+                             int k, int grid, cudaStream_t st, int post) {
 #define BPK_LAUNCH(D, O)                                                                              \
     if (dim == D && order == O) {                                                                     \
-        if (v) k_phase<D, O, P, true><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k);         \
-        else k_phase<D, O, P, false><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k);          \
+        if (v) k_phase<D, O, P, true><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, 0);      \
+        else k_phase<D, O, P, false><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, post);    \
         return cudaGetLastError();                                                                    \
     }
         BPK_LAUNCH(2, 2) BPK_LAUNCH(2, 4) BPK_LAUNCH(3, 2) BPK_LAUNCH(3, 4)
@@ -892,10 +940,10 @@ struct Launch {
 // C++ entry points used by the host code (sim.cu, batch.cu).
 namespace bpk {
 cudaError_t launch_phase(int prec, int dim, int order, bool vphase, const ShotDesc* d_shots, int nshots,
-                         long long ntiles, int k, int grid, cudaStream_t st) {
-    if (prec == BP_PREC_FP32) return Launch<PolF32>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st);
-    if (prec == BP_PREC_COMP16) return Launch<PolC16>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st);
-    return Launch<PolF64>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st);
+                         long long ntiles, int k, int grid, cudaStream_t st, int post) {
+    if (prec == BP_PREC_FP32) return Launch<PolF32>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post);
+    if (prec == BP_PREC_COMP16) return Launch<PolC16>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post);
+    return Launch<PolF64>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post);
 }
 
 cudaError_t launch_post(int prec, const ShotDesc* d_shots, int nshots, int max_rec, int k, int do_record,
