@@ -260,7 +260,8 @@ int bp_profile_phases(bp_sim* sim, int nsteps, float ms[3]);
  * numerator) and the number of updated cells per step. */
 int bp_algorithmic_bytes(bp_sim* sim, double bytes_per_cell[2], long long* cells);
 
-/* Kernel launches one step issues (for launch counting). */
+/* Kernel launches one step issues (for launch counting): 3 (V phase, T phase,
+ * record/inject), or 2 where the T phase records and injects itself. */
 int bp_launches_per_step(bp_sim* sim, int* n);
 /* Kernel launches this simulation has issued so far (graph replays count
  * every kernel node they contain). */

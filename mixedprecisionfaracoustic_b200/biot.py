@@ -271,6 +271,13 @@ class Simulation:
         check(self.lib.bp_algorithmic_bytes(self.h, b, C.byref(cells)), "bp_algorithmic_bytes")
         return (b[0], b[1]), cells.value
 
+    def launches_per_step(self) -> int:
+        """Kernels one step launches: 3, or 2 where the T phase records the
+        receivers and injects the source itself."""
+        n = C.c_int()
+        check(self.lib.bp_launches_per_step(self.h, C.byref(n)), "bp_launches_per_step")
+        return n.value
+
     def launch_count(self) -> int:
         n = C.c_longlong()
         check(self.lib.bp_launch_count(self.h, C.byref(n)), "bp_launch_count")

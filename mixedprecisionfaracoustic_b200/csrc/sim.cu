@@ -496,7 +496,7 @@ int bp_algorithmic_bytes(bp_sim* s, double bpc[2], long long* cells) {
 
 int bp_launches_per_step(bp_sim* s, int* n) {
     if (!s || !n) { set_error("bad arguments"); return BP_ERR_ARG; }
-    *n = 3;
+    *n = s->run.launches_per_step();
     return BP_OK;
 }
 

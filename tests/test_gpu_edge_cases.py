@@ -124,6 +124,7 @@ def test_recording_in_the_t_phase_equals_the_post_kernel(dim, prec):
     border.rec_y = list(cfg.rec_y) + [cfg.rec_y[0]]
     border.rec_z = list(cfg.rec_z) + [0]
     with Simulation(cfg, med) as a, Simulation(border, med) as b:
+        assert (a.launches_per_step(), b.launches_per_step()) == (2, 3)
         a.run(cfg.nt)
         b.run(cfg.nt)
         a.sync()
