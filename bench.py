@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--nz", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=20)
+    ap.add_argument("--min-timed-s", type=float, default=1.0,
+                    help="c1: repeat the K-step timed region until the repetitions cover this many seconds")
+    ap.add_argument("--no-batched", action="store_true", help="c1 line: skip the full-size c3 batched object")
     ap.add_argument("--workload", choices=["c0", "c1", "c2", "c3", "c4"], default="c1",
                     help="c1: one 2D shot (default, the headline); c0: the 3D 160^3 order-4 homogeneous shot; "
                          "c2: one 3D 512x512x384 shot; c3: 64 batched 2D shots; c4: serving stream")
@@ -132,9 +135,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def workload(precision, nt, nx, nz):
+def workload(precision, nt, nx, nz, host=False):
+    """The c1 shot; host=True forms its medium without loading the CUDA library
+    (the reference arm), with values bit-identical to the library's."""
     from mixedprecisionfaracoustic_b200.presets import config1
-    return config1(precision=precision, seed=1, nx=nx, nz=nz, nt=nt)
+    return config1(precision=precision, seed=1, nx=nx, nz=nz, nt=nt, host=host)
+
+
+def c1_config(args, ws):
+    """The `config` object of the c1 line, the same in both arms."""
+    return {"workload": WORKLOAD, "grid": [args.nx + 40, args.nz + 40], "order": 2,
+            "global_batch": ws, "seq_len": None, "parallelism": f"replicas x{ws}",
+            "l2_flush": "inputs larger than L2 (1.0 GB working set)"}
 
 
 def ncu_traffic():
@@ -148,30 +160,50 @@ def ncu_traffic():
     return {}
 
 
+C1_STEPS = 8000          # c1's configured run length
+
+
 def run_ours(args, rank, ws):
+    """The c1 line: FP32 (headline) and COMP16 on one shot per GPU.  The timed
+    region is K steps bracketed by a barrier and events on the library's
+    stream; it is repeated R times (the same R on every rank) so that the
+    repetitions cover at least --min-timed-s seconds, and the median region
+    gives the per-step time.  Then the FP64 run of the same steps (seismogram
+    rel-L2), the per-phase profile, and e2e: the whole configured c1 job
+    through the public API."""
     import torch
     from mixedprecisionfaracoustic_b200 import Simulation
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     K, W, P = args.steps, args.warmup, args.profile_steps
-    nt = W + K + P
     peak, peak_kind = measured_peaks()
     res = {}
     sims = {}
+    reps = None
     precs = (args.only,) if args.only else ("fp32", "comp16")
     for prec in precs:
-        cfg, med = workload(prec, nt, args.nx, args.nz)
+        cfg, med = workload(prec, max(C1_STEPS, W + K + P), args.nx, args.nz)
         cfg.device = dev
         s = Simulation(cfg, med)
-        s.run(W)
-        s.sync()
-        if ws > 1:
-            torch.distributed.barrier()
+        ms_w = s.run_timed(W)
+        if reps is None:
+            per = max(ms_w / max(W, 1), 1e-4)
+            reps = max(1, int(np.ceil(args.min_timed_s * 1e3 / (K * per))))
+            reps = max(1, min(reps, (cfg.nt - W - P) // K))
+            if ws > 1:
+                t = torch.tensor([reps], device="cuda", dtype=torch.int64)
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                reps = int(t.item())
         l0 = s.launch_count()
+        regions = []
         with ClockSampler(dev) as clk:
-            ms = s.run_timed(K)
-        launches = s.launch_count() - l0
+            for _ in range(reps):
+                if ws > 1:
+                    torch.distributed.barrier()
+                regions.append(s.run_timed(K))
+        launches = (s.launch_count() - l0) // reps
+        ms = float(np.median(regions))
         if ws > 1:
             t = torch.tensor([ms], device="cuda", dtype=torch.float64)
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -185,6 +217,8 @@ def run_ours(args, rank, ws):
         res[prec] = {
             "value": cells * K * ws / (ms * 1e-3) / 1e6,
             "ms_per_step": ms / K,
+            "timed_regions": {"count": reps, "steps_each": K, "ms_min": min(regions), "ms_median": ms,
+                              "ms_max": max(regions)},
             "launches": launches,
             "clocks": clk.summary(),
             "phase_ms": {"v_phase": pv, "t_phase": pt, "record_inject": pp},
@@ -200,18 +234,21 @@ def run_ours(args, rank, ws):
             s.close()
         return res, None
     # FP64 run of the same steps: seismogram relative L2 of both paths
-    cfg, med = workload("fp64", nt, args.nx, args.nz)
+    steps_run = W + reps * K + P
+    cfg, med = workload("fp64", max(C1_STEPS, W + K + P), args.nx, args.nz)
     cfg.device = dev
     s64 = Simulation(cfg, med)
-    s64.run(W + K + P)
+    s64.run(steps_run)
     s64.sync()
     for prec in ("fp32", "comp16"):
-        res[prec]["rel_l2_vs_fp64"] = {c: sims[prec].trace_rel_l2(s64, c) for c in ("txx", "tzz", "vux", "p")}
+        res[prec]["rel_l2_vs_fp64"] = {c: sims[prec].trace_rel_l2(s64, c) for c in ("txx", "tzz", "vux", "vwx", "p")}
+        res[prec]["rel_l2_steps"] = steps_run
     s64.close()
     for s in sims.values():
         s.close()
-    # end to end through the public API: pinned host medium in, traces out
-    cfg, med = workload("fp32", K, args.nx, args.nz)
+    # end to end through the public API: the whole configured c1 job (8000
+    # steps), pinned host medium in, the five seismograms out into pinned buffers
+    cfg, med = workload("fp32", C1_STEPS, args.nx, args.nz)
     cfg.device = dev
     pinned = {}
     for k, v in med.items():
@@ -221,13 +258,12 @@ def run_ours(args, rank, ws):
     from mixedprecisionfaracoustic_b200.biot import Medium
     pm = Medium(pinned)
     h2d = sum(a.nbytes for a in pinned.values())
-    # pinned host buffers for the seismograms, like the medium's
-    outs = [torch.empty((cfg.nrec, K), dtype=torch.float32, pin_memory=True).numpy() for _ in range(5)]
+    outs = [torch.empty((cfg.nrec, cfg.nt), dtype=torch.float32, pin_memory=True).numpy() for _ in range(5)]
     if ws > 1:
         torch.distributed.barrier()
     t0 = time.perf_counter()
     s = Simulation(cfg, pm)
-    s.run(K)
+    s.run(cfg.nt)
     tr = [s.traces(c, out=o) for c, o in zip(("txx", "tzz", "vux", "vwx", "p"), outs)]
     s.close()
     e2e_s = time.perf_counter() - t0
@@ -236,10 +272,47 @@ def run_ours(args, rank, ws):
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = {"value": res["fp32"]["cells"] * K * ws / e2e_s / 1e6, "unit": METRIC,
-           "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K, "seconds": e2e_s,
-           "path": "bp_create(pinned host medium) + bp_run(K) + bp_get_traces x5 + bp_destroy"}
+    e2e = {"value": res["fp32"]["cells"] * cfg.nt * ws / e2e_s / 1e6, "unit": METRIC,
+           "h2d_bytes_per_step": h2d / cfg.nt, "d2h_bytes_per_step": d2h / cfg.nt, "steps": cfg.nt,
+           "seconds": e2e_s,
+           "path": f"bp_create(pinned host medium) + bp_run({cfg.nt}) + bp_get_traces x5 + bp_destroy: "
+                   f"the whole c1 job"}
     return res, e2e
+
+
+def run_batched(args):
+    """c3 at full size in the default line: 64 2D shots (sizes from {1024^2,
+    1536x1024, 2048^2, 3072x1536}, seed 3), one persistent launch per phase for
+    all shots, FP32 and COMP16.  The autotuner runs first (its steps are real
+    steps of the shots, outside the timed region); then max(K, 100) steps are
+    timed with CUDA events on the batch's stream."""
+    from mixedprecisionfaracoustic_b200 import Batch
+    from mixedprecisionfaracoustic_b200.presets import config3_shots
+    K = max(args.steps, 100)
+    tune_budget = 800
+    shots = config3_shots(seed=3, nshots=64, nt=4000, precision="fp32")
+    cells = sum((c.padded[0] - 2) * (c.padded[2] - 2) for c, _ in shots)
+    peak, peak_kind = measured_peaks()
+    out = {"workload": "c3: 64 batched 2D shots at full size (seed 3), order 2, 4000-step shots",
+           "cells_per_step": cells, "timed_steps": K}
+    for prec, bpc in (("fp32", 144.0), ("comp16", 108.0)):
+        for c, _ in shots:
+            c.precision = prec
+        b = Batch([c for c, _ in shots], [m for _, m in shots])
+        tune = b.autotune(tune_budget)
+        b.run(max(args.warmup, 3))
+        b.sync()
+        with ClockSampler(0) as clk:
+            ms = b.run_timed(K)
+        b.sync()
+        got = bpc * cells * K / (ms * 1e-3) / 1e9
+        out[prec] = {"value": cells * K / (ms * 1e-3) / 1e6, "unit": METRIC, "ms_per_step": ms / K,
+                     "tune": tune, "clocks": clk.summary(),
+                     "roofline": {"bound": "hbm", "kernel": "step", "bytes_per_cell": bpc, "achieved": got,
+                                  "peak": peak, "unit": "GB/s", "frac": got / peak, "peak_source": peak_kind}}
+        b.close()
+    out["speedup_comp16_vs_fp32"] = out["comp16"]["value"] / out["fp32"]["value"]
+    return out
 
 
 def cpu_baseline(args, budget_s=20.0):
@@ -247,7 +320,7 @@ def cpu_baseline(args, budget_s=20.0):
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     O.set_threads(threads)
-    cfg, med = workload("fp32", 8, args.nx, args.nz)
+    cfg, med = workload("fp32", 8, args.nx, args.nz, host=True)
     probe = O.Oracle(cfg, med, O.REF32)
     probe.run(2)
     t0 = time.perf_counter()
@@ -255,7 +328,7 @@ def cpu_baseline(args, budget_s=20.0):
     per = (time.perf_counter() - t0) / 3
     probe.close()
     n = int(max(3, budget_s / max(per, 1e-6)))
-    cfg, med = workload("fp32", n + 4, args.nx, args.nz)
+    cfg, med = workload("fp32", n + 4, args.nx, args.nz, host=True)
     o = O.Oracle(cfg, med, O.REF32)
     o.run(2)
     t0 = time.perf_counter()
@@ -269,13 +342,15 @@ def cpu_baseline(args, budget_s=20.0):
 
 
 def run_reference(args, rank, ws):
-    """Reference arm: the reference's update equations on the host cores."""
+    """Reference arm: the reference's update equations (the oracle's REF32
+    arithmetic) on all host cores, on the same c1 workload.  Nothing here loads
+    the CUDA library: the medium is formed on the host."""
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     O.set_threads(threads)
     K, W = args.steps, args.warmup
     nz = args.nz
-    cfg, med = workload("fp32", 4, args.nx, nz)
+    cfg, med = workload("fp32", 4, args.nx, nz, host=True)
     probe = O.Oracle(cfg, med, O.REF32)
     probe.run(1)
     t0 = time.perf_counter()
@@ -285,7 +360,7 @@ def run_reference(args, rank, ws):
     budget = 150.0
     if (K + W) * per_full > budget:      # bounded sample: fewer rows, same nx and medium statistics
         nz = max(64, int(nz * budget / ((K + W) * per_full)))
-    cfg, med = workload("fp32", K + W + 1, args.nx, nz)
+    cfg, med = workload("fp32", K + W + 1, args.nx, nz, host=True)
     o = O.Oracle(cfg, med, O.REF32)
     o.run(W)
     t0 = time.perf_counter()
@@ -297,7 +372,7 @@ def run_reference(args, rank, ws):
     return {"metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus, "steps": K, "warmup": W,
             "ms_per_step": el / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "global_batch": 1, "seq_len": None, "parallelism": "replicas"},
+            "config": c1_config(args, ws),
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -578,6 +653,7 @@ def main():
         print(json.dumps({"metric": METRIC, "only": args.only, **res[args.only]}), flush=True)
     elif rank == 0:
         f32, c16 = res["fp32"], res["comp16"]
+        batched = None if (args.no_batched or ws > 1) else run_batched(args)
         cpu = None if (args.no_cpu_baseline or ws > 1) else cpu_baseline(args)
         traffic = ncu_traffic()
         roof = dict(f32["roofline"])
@@ -589,20 +665,21 @@ def main():
             "metric": METRIC, "value": f32["value"], "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": f32["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": [args.nx + 40, args.nz + 40], "order": 2,
-                       "global_batch": ws, "seq_len": None, "parallelism": f"replicas x{ws}",
-                       "l2_flush": "inputs larger than L2 (1.0 GB working set)"},
+            "config": c1_config(args, ws),
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": f32["launches"],
             "clocks": f32["clocks"],
             "rel_l2_vs_fp64": f32["rel_l2_vs_fp64"],
+            "timed_regions": f32["timed_regions"],
             "phase_ms": f32["phase_ms"],
             "comp16": {"value": c16["value"], "ms_per_step": c16["ms_per_step"], "roofline": c16roof,
                        "rel_l2_vs_fp64": c16["rel_l2_vs_fp64"], "phase_ms": c16["phase_ms"],
                        "gpu_launches": c16["launches"], "clocks": c16["clocks"],
+                       "timed_regions": c16["timed_regions"],
                        "speedup_vs_fp32": c16["value"] / f32["value"]},
+            "batched": batched,
         }
         print(json.dumps(out), flush=True)
     if ws > 1:

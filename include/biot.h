@@ -46,6 +46,16 @@ extern "C" {
 #define BP_PREC_COMP16 1    /* fp16 hi + int8 residual storage, fp32 math     */
 #define BP_PREC_FP64 2      /* fp64 storage and arithmetic (accuracy reference) */
 
+/* FP32 rounding (bp_config.rounding).  FAST divides by H with a reciprocal and
+ * one residual step (within one ulp of the IEEE quotient) and forms the CPML
+ * memory update in float.  REFERENCE rounds both like the reference's Float
+ * build (Float/main.cu:115-158,234-285): the IEEE quotient by H, and psi e +
+ * b (e prev + d) with one rounding after the float product psi e, as its
+ * double-promoted expression gives.  REFERENCE runs the register tile kernels
+ * only and applies to FP32 only. */
+#define BP_ROUND_FAST 0
+#define BP_ROUND_REFERENCE 1
+
 /* wavefield components, in the order used for bp_get_field / snapshots */
 #define BP_F_VUX 0
 #define BP_F_VUY 1
@@ -104,7 +114,8 @@ typedef struct bp_config {
     int comp_coef_lo;     /* COMP16: 1 = coefficients keep an int8 residual too   */
     int dyn_scale;        /* COMP16: 1 = ramp the state scale 1 -> 16 (Half/main.cu:116-122) */
     int check_cfl;        /* 1 = refuse dt above the stability limit (BP_ERR_CFL) */
-    int reserved[4];
+    int rounding;         /* FP32: BP_ROUND_FAST (0) or BP_ROUND_REFERENCE (1)   */
+    int reserved[3];
 } bp_config;
 
 /* Cell-centred Biot coefficients over the PHYSICAL grid (nz*ny*nx floats each,
@@ -279,11 +290,16 @@ int bp_comp16_decode(const uint16_t* hi, const int8_t* lo, size_t n, float* out)
  * its reduction scratch on the device for the duration of the call. */
 int bp_rel_l2_device(const float* d_x, const float* d_ref, size_t n, double* rel);
 /* The same quantity without any device allocation (no counterpart in the
- * reference).  The reduction scratch is a fixed 16 KB array in the library's
- * device image, so n is limited to 16,777,216 elements (larger n returns
- * BP_ERR_ARG).  The first call on a device, with that device current, looks up
- * the array's address; make it before any stream capture begins.  Calls share
- * that array: concurrent calls on one device race and must be serialised. */
+ * reference), for callers that cannot allocate: real-time loops that must not
+ * stall on cudaMalloc's implicit synchronisation, and processes that reserve
+ * all device memory for their own pool.  The reduction scratch is a fixed 16 KB
+ * array in the library's device image, so n is limited to 16,777,216 elements
+ * (larger n returns BP_ERR_ARG).  The call is synchronous (legacy default
+ * stream, blocking read-back of the result); the inputs must be complete, so
+ * synchronise the stream that produces them first.  The first call on a
+ * device, with that device current, looks up the array's address; make it
+ * before any stream capture begins.  Calls share that array: concurrent calls
+ * on one device race and must be serialised. */
 int bp_rel_l2_device_noalloc(const float* d_x, const float* d_ref, size_t n, double* rel);
 /* Relative L2 seismogram error of component comp of `x` against `ref` (same
  * receivers and nt), computed on the device in FP64. */
@@ -299,6 +315,13 @@ void bp_destroy(bp_sim* sim);
  * is emptied when an allocation fails.  This call returns it to the system
  * for one device, or for all with device = -1. */
 int bp_release_cached_memory(int device);
+
+/* Test hook (no counterpart in the reference): the nth device-memory request
+ * the library makes from now on (1 = the next one; every arena block, cached
+ * or new, counts) fails as if the device were out of memory, so tests can
+ * drive the BP_ERR_OOM paths of bp_create, bp_batch_create and the server's
+ * admission without exhausting a GPU.  0 disarms.  Process-wide. */
+int bp_debug_fail_allocation(int nth);
 
 const char* bp_error_string(int code);
 const char* bp_last_error(void);
@@ -327,10 +350,14 @@ int bp_cfl_limit(const bp_config* cfg, const bp_medium* medium, double* dt_max,
 typedef struct bp_batch bp_batch;
 
 typedef struct bp_tune {
-    int tile_rows;        /* rows (z, or y*z in 3D) per tile; 0 = autotune      */
+    int tile_rows;        /* rows (z, or y*z in 3D) per tile of the register
+                             kernels, a power of two 4..32; 0 = autotune      */
     int steps_per_sync;   /* steps captured per CUDA graph launch; 0 = autotune */
     int ctas_per_sm;      /* persistent CTAs per SM; 0 = autotune               */
-    int reserved[5];
+    int tile_segs;        /* 128-cell x segments per tile, 1..4 (0 = 1)        */
+    int tile_tz;          /* 3D: z planes among the tile's rows, 1..tile_rows
+                             (0 = the precision's default)                    */
+    int reserved[3];
 } bp_tune;
 
 /* All shots must share dim, order and precision; sizes, media, sources and
@@ -340,8 +367,20 @@ int bp_batch_create(const bp_config* cfgs, const bp_medium* media, int nshots,
 /* Advances every unfinished shot by up to nsteps steps (async). */
 int bp_batch_run(bp_batch* b, int nsteps);
 int bp_batch_sync(bp_batch* b);
+/* bp_batch_run bracketed by CUDA events on the batch's stream; waits and
+ * returns the device time of the steps in *ms (the autotuner, if it still has
+ * to run, runs first, outside the timed region). */
+int bp_batch_run_timed(bp_batch* b, int nsteps, float* ms);
 int bp_batch_get_traces(bp_batch* b, int shot, int comp, float* host, size_t n);
 int bp_batch_get_tune(bp_batch* b, bp_tune* chosen);
+/* Runs the autotuner now (it otherwise runs inside the first bp_batch_run):
+ * times real steps of the batch, at most budget_steps of them, under candidate
+ * tile shapes, then persistent CTAs per SM, then steps per sync, and keeps
+ * the fastest; results are cached per (dim, order, precision, rounding, grid
+ * class) for the process.  The timed steps advance the shots.  No-op when the
+ * bp_tune given to bp_batch_create fixed every setting.  (No counterpart in
+ * the reference, which has one fixed (16, 8, 1) block, Float/main.cu:26-28.) */
+int bp_batch_autotune(bp_batch* b, int budget_steps);
 /* Total cell-updates performed so far (all shots). */
 int bp_batch_cell_updates(bp_batch* b, long long* updates);
 void bp_batch_destroy(bp_batch* b);

@@ -21,6 +21,7 @@ FIELD = {n: i for i, n in enumerate(FIELDS)}
 TRACES = ["txx", "tzz", "vux", "vwx", "p"]          # sisx sisz sisvu sisvw sisp
 TRACE = {n: i for i, n in enumerate(TRACES)}
 SRC_TAU, SRC_P = 1, 2
+ROUND = {"fast": 0, "reference": 1}
 KERNELS = {"auto": 0, "register": 1, "staged": 2, "march": 3}
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 COEFS = ["rho_x", "rho_y", "rho_z", "rhof", "cc1_x", "cc1_y", "cc1_z", "cc2_x", "cc2_y", "cc2_z",
@@ -43,7 +44,7 @@ class BpConfig(C.Structure):
         ("nrec", C.c_int), ("rec_x", IntP), ("rec_y", IntP), ("rec_z", IntP),
         ("nsnap", C.c_int), ("snap_steps", IntP), ("snap_fields", C.c_uint), ("snap_masks", UIntP),
         ("snap_y", C.c_int), ("device", C.c_int), ("comp_coef_lo", C.c_int), ("dyn_scale", C.c_int),
-        ("check_cfl", C.c_int), ("reserved", C.c_int * 4),
+        ("check_cfl", C.c_int), ("rounding", C.c_int), ("reserved", C.c_int * 3),
     ]
 
 
@@ -53,7 +54,7 @@ class BpMedium(C.Structure):
 
 class BpTune(C.Structure):
     _fields_ = [("tile_rows", C.c_int), ("steps_per_sync", C.c_int), ("ctas_per_sm", C.c_int),
-                ("reserved", C.c_int * 5)]
+                ("tile_segs", C.c_int), ("tile_tz", C.c_int), ("reserved", C.c_int * 3)]
 
 
 class BpServerStats(C.Structure):
@@ -101,6 +102,7 @@ _SIGS = [
     ("bp_trace_rel_l2", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, DoubleP]),
     ("bp_destroy", None, [C.c_void_p]),
     ("bp_release_cached_memory", C.c_int, [C.c_int]),
+    ("bp_debug_fail_allocation", C.c_int, [C.c_int]),
     ("bp_error_string", C.c_char_p, [C.c_int]),
     ("bp_last_error", C.c_char_p, []),
     ("bp_medium_reference_borehole", C.c_int, [C.c_int, C.c_int, C.c_int, FloatP]),
@@ -110,8 +112,10 @@ _SIGS = [
                                   C.POINTER(C.c_void_p)]),
     ("bp_batch_run", C.c_int, [C.c_void_p, C.c_int]),
     ("bp_batch_sync", C.c_int, [C.c_void_p]),
+    ("bp_batch_run_timed", C.c_int, [C.c_void_p, C.c_int, FloatP]),
     ("bp_batch_get_traces", C.c_int, [C.c_void_p, C.c_int, C.c_int, FloatP, C.c_size_t]),
     ("bp_batch_get_tune", C.c_int, [C.c_void_p, C.POINTER(BpTune)]),
+    ("bp_batch_autotune", C.c_int, [C.c_void_p, C.c_int]),
     ("bp_batch_cell_updates", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     ("bp_batch_destroy", None, [C.c_void_p]),
     ("bp_shot_bytes", C.c_int, [C.POINTER(BpConfig), C.POINTER(C.c_size_t)]),

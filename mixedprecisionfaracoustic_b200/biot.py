@@ -52,6 +52,7 @@ class ShotConfig:
     comp_coef_lo: int = 1
     dyn_scale: int = 1
     check_cfl: int = 0
+    rounding: str = "fast"                # FP32: "fast" or "reference" (bp_config.rounding)
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -87,6 +88,7 @@ class ShotConfig:
             c.snap_masks = sm.ctypes.data_as(_abi.UIntP)
         c.snap_y = self.snap_y
         c.device, c.comp_coef_lo, c.dyn_scale, c.check_cfl = self.device, self.comp_coef_lo, self.dyn_scale, self.check_cfl
+        c.rounding = _abi.ROUND[self.rounding]
         return c
 
 
@@ -327,13 +329,18 @@ class Batch:
     """Many shots advanced by the same launches (bp_batch)."""
 
     def __init__(self, cfgs: Sequence[ShotConfig], media: Sequence[Medium], steps_per_sync: int = 0,
-                 ctas_per_sm: int = 0):
+                 ctas_per_sm: int = 0, tile: Optional[tuple] = None):
+        """tile = (rows, segs[, tz]) fixes the register kernels' tile shape;
+        None leaves it (and any other 0 setting) to the autotuner."""
         self.lib = load()
         self.cfgs = list(cfgs)
         carr = (BpConfig * len(cfgs))(*[c.to_c() for c in cfgs])
         marr = (BpMedium * len(media))(*[m.to_c() for m in media])
         t = BpTune()
         t.steps_per_sync, t.ctas_per_sm = steps_per_sync, ctas_per_sm
+        if tile is not None:
+            t.tile_rows, t.tile_segs = tile[0], tile[1]
+            t.tile_tz = tile[2] if len(tile) > 2 else 0
         h = C.c_void_p()
         check(self.lib.bp_batch_create(carr, marr, len(cfgs), C.byref(t), C.byref(h)), "bp_batch_create")
         self.h = h
@@ -343,6 +350,12 @@ class Batch:
 
     def sync(self) -> None:
         check(self.lib.bp_batch_sync(self.h), "bp_batch_sync")
+
+    def run_timed(self, nsteps: int) -> float:
+        """Runs nsteps and returns their device time in ms (CUDA events on the batch's stream)."""
+        ms = C.c_float()
+        check(self.lib.bp_batch_run_timed(self.h, int(nsteps), C.byref(ms)), "bp_batch_run_timed")
+        return ms.value
 
     def traces(self, shot: int, comp) -> np.ndarray:
         ci = _abi.TRACE[comp] if isinstance(comp, str) else int(comp)
@@ -354,7 +367,13 @@ class Batch:
     def tune(self) -> dict:
         t = BpTune()
         check(self.lib.bp_batch_get_tune(self.h, C.byref(t)), "bp_batch_get_tune")
-        return {"tile_rows": t.tile_rows, "steps_per_sync": t.steps_per_sync, "ctas_per_sm": t.ctas_per_sm}
+        return {"tile_rows": t.tile_rows, "tile_segs": t.tile_segs, "tile_tz": t.tile_tz,
+                "steps_per_sync": t.steps_per_sync, "ctas_per_sm": t.ctas_per_sm}
+
+    def autotune(self, budget_steps: int) -> dict:
+        """Runs the autotuner now within budget_steps (real) steps; returns the choice."""
+        check(self.lib.bp_batch_autotune(self.h, int(budget_steps)), "bp_batch_autotune")
+        return self.tune()
 
     def cell_updates(self) -> int:
         n = C.c_longlong()

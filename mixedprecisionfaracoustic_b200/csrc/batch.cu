@@ -48,13 +48,15 @@ int BatchCore::rebuild() {
     long long t0 = 0;
     int maxrec = 0;
     long long t0s = 0, t0m = 0;
+    const TileShape ts = effective_shape();
     for (int i = 0; i < n; i++) {
         h[i] = shots[i]->desc;
+        const long long tiles = apply_tile_shape(h[i], dim, prec, ts);
         h[i].tile0 = t0;
         h[i].tile0s = t0s;
         h[i].tile0m = t0m;
         h[i].done = 0;
-        t0 += shots[i]->ntiles;
+        t0 += tiles;
         t0s += shots[i]->ntiles_s;
         t0m += shots[i]->ntiles_m;
         maxrec = std::max(maxrec, shots[i]->nurec);
@@ -66,6 +68,8 @@ int BatchCore::rebuild() {
     }
     run.post_in_t = true;
     for (auto& sh : shots) run.post_in_t = run.post_in_t && sh->post_in_t;
+    run.rounding = rounding;
+    run.multi_unit = ts.rows * ts.segs > phase_threads() / 32;
     run.configure(prec, dim, order, d_descs, n, t0, t0s, t0m, maxrec, st, ctas_per_sm,
                   steps_per_sync > 0 ? steps_per_sync : 32);
     return BP_OK;
@@ -87,61 +91,106 @@ int BatchCore::advance(int n) {
     return BP_OK;
 }
 
+TileShape BatchCore::effective_shape() const {
+    return shape.rows > 0 ? shape : default_tile_shape(dim, prec);
+}
+
+// Tile shapes the autotuner tries (the default first).  2D: rows x segments;
+// 3D also the split of the rows into y rows x z planes.
+static std::vector<TileShape> shape_candidates(int dim, int prec) {
+    std::vector<TileShape> c = {default_tile_shape(dim, prec)};
+    auto add = [&](int rows, int segs, int tz) {
+        TileShape t{rows, segs, tz};
+        for (auto& o : c)
+            if (o.rows == t.rows && o.segs == t.segs && (dim == 2 || o.tz == t.tz)) return;
+        c.push_back(t);
+    };
+    if (dim == 2) {
+        add(4, 2, 1); add(16, 1, 1); add(8, 2, 1); add(4, 1, 1);
+    } else {
+        add(8, 1, 1); add(8, 1, 2); add(8, 1, 4); add(8, 1, 8); add(16, 1, 4); add(16, 1, 8); add(4, 2, 2);
+    }
+    return c;
+}
+
 int BatchCore::autotune(int budget_steps) {
     if (shots.empty()) return BP_OK;
     long long cells = total_cells();
-    TuneKey key{dim, order, prec, (int)std::floor(std::log2((double)std::max(cells, 1LL)))};
+    TuneKey key{dim, order, prec + 16 * rounding, (int)std::floor(std::log2((double)std::max(cells, 1LL))),
+                (int)std::floor(std::log2((double)shots.size()))};
+    const bool fix_shape = shape.rows > 0, fix_c = ctas_per_sm > 0, fix_s = steps_per_sync > 0;
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         auto it = tune_cache().find(key);
         if (it != tune_cache().end()) {
-            if (ctas_per_sm == 0) ctas_per_sm = it->second.ctas_per_sm;
-            if (steps_per_sync == 0) steps_per_sync = it->second.steps_per_sync;
+            if (!fix_c) ctas_per_sm = it->second.ctas_per_sm;
+            if (!fix_s) steps_per_sync = it->second.steps_per_sync;
+            if (!fix_shape) shape = it->second.shape;
             tuned = true;
             return rebuild();
         }
     }
-    const int occ = std::min(phase_occupancy(prec, dim, order, true), phase_occupancy(prec, dim, order, false));
-    std::vector<int> ctas = {0};
-    if (occ >= 2) ctas.push_back(occ / 2 > 0 ? occ / 2 : 1);
-    if (occ >= 3) ctas.push_back(1);
-    std::vector<int> spss = {8, 32, 128};
-    if (ctas_per_sm > 0) ctas = {ctas_per_sm};
-    if (steps_per_sync > 0) spss = {steps_per_sync};
     int min_left = 1 << 30;
     for (auto& s : shots) min_left = std::min(min_left, s->cfg.nt - s->it_host);
-    const int fixed_c = ctas_per_sm, fixed_s = steps_per_sync;
-    double best = 1e30;
-    TuneVal bv{fixed_c, fixed_s > 0 ? fixed_s : 32};
+    const int budget = std::min(budget_steps, min_left);
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     int used = 0;
-    for (int c : ctas) {
-        for (int sps : spss) {
-            const int steps = std::max(sps, 16);
-            if (used + 2 * steps > std::min(budget_steps, min_left)) continue;
-            ctas_per_sm = c;
-            steps_per_sync = sps;
-            int rc = rebuild();
-            if (rc) { cudaEventDestroy(a); cudaEventDestroy(b); return rc; }
-            advance(sps);                          // warm: captures the graph
-            cudaEventRecord(a, st);
-            rc = advance(steps);
-            cudaEventRecord(b, st);
-            cudaEventSynchronize(b);
-            used += sps + steps;
-            if (rc) { cudaEventDestroy(a); cudaEventDestroy(b); return rc; }
-            float ms = 0;
-            cudaEventElapsedTime(&ms, a, b);
-            const double per = ms / steps;
-            if (per < best) { best = per; bv = TuneVal{c, sps}; }
-        }
+    double best = 1e30;
+    TuneVal bv{ctas_per_sm, fix_s ? steps_per_sync : 32, effective_shape()};
+    // times one candidate; false if it no longer fits the step budget
+    auto trial = [&](int c, int sps, TileShape ts, int* rc) -> bool {
+        const int steps = std::max(sps, 16);
+        if (used + sps + steps > budget) return false;
+        ctas_per_sm = c;
+        steps_per_sync = sps;
+        shape = ts;
+        *rc = rebuild();
+        if (*rc) return false;
+        advance(sps);                          // warm: captures the graph
+        cudaEventRecord(a, st);
+        *rc = advance(steps);
+        cudaEventRecord(b, st);
+        cudaEventSynchronize(b);
+        used += sps + steps;
+        if (*rc) return false;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        const double per = ms / steps;
+        if (per < best) { best = per; bv = TuneVal{c, sps, ts}; }
+        return true;
+    };
+    int rc = BP_OK;
+    // stage 1: tile shape (at the current CTA count and 32 steps per sync)
+    if (!fix_shape)
+        for (const TileShape& ts : shape_candidates(dim, prec))
+            if (!trial(bv.ctas_per_sm, bv.steps_per_sync, ts, &rc) && rc) break;
+    // stage 2: persistent CTAs per SM
+    if (!rc && !fix_c) {
+        const int occ = std::min(phase_occupancy(prec, dim, order, true, rounding),
+                                 phase_occupancy(prec, dim, order, false, rounding));
+        std::vector<int> ctas = {0};
+        if (occ >= 2) ctas.push_back(occ / 2 > 0 ? occ / 2 : 1);
+        if (occ >= 3) ctas.push_back(1);
+        const TuneVal base = bv;
+        for (int c : ctas)
+            if (!(c == base.ctas_per_sm && !fix_shape && best < 1e30))
+                if (!trial(c, base.steps_per_sync, base.shape, &rc) && rc) break;
+    }
+    // stage 3: steps per graph replay
+    if (!rc && !fix_s) {
+        const TuneVal base = bv;
+        for (int sps : {8, 32, 128})
+            if (sps != base.steps_per_sync || best >= 1e30)
+                if (!trial(base.ctas_per_sm, sps, base.shape, &rc) && rc) break;
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    if (rc) return rc;
     ctas_per_sm = bv.ctas_per_sm;
     steps_per_sync = bv.steps_per_sync;
+    shape = bv.shape;
     tuned = true;
     if (best < 1e30) {
         std::lock_guard<std::mutex> g(g_tune_mu);
@@ -172,6 +221,8 @@ struct bp_batch {
 
 extern "C" {
 
+int bp_batch_autotune(bp_batch* b, int budget_steps);
+
 int bp_batch_create(const bp_config* cfgs, const bp_medium* media, int nshots, const bp_tune* tune, bp_batch** out) {
     if (!cfgs || !media || nshots < 1 || !out) { set_error("bad arguments"); return BP_ERR_ARG; }
     *out = nullptr;
@@ -179,8 +230,8 @@ int bp_batch_create(const bp_config* cfgs, const bp_medium* media, int nshots, c
         int rc = validate_config(&cfgs[i]);
         if (rc) return rc;
         if (cfgs[i].dim != cfgs[0].dim || cfgs[i].order != cfgs[0].order || cfgs[i].precision != cfgs[0].precision ||
-            cfgs[i].device != cfgs[0].device) {
-            set_error("all shots of a batch share dim, order, precision and device");
+            cfgs[i].device != cfgs[0].device || cfgs[i].rounding != cfgs[0].rounding) {
+            set_error("all shots of a batch share dim, order, precision, rounding and device");
             return BP_ERR_ARG;
         }
     }
@@ -197,10 +248,21 @@ int bp_batch_create(const bp_config* cfgs, const bp_medium* media, int nshots, c
     b->core.dim = cfgs[0].dim;
     b->core.order = cfgs[0].order;
     b->core.prec = cfgs[0].precision;
+    b->core.rounding = cfgs[0].rounding;
     if (tune) {
+        if (tune->tile_rows > 0) {
+            TileShape t{tune->tile_rows, tune->tile_segs > 0 ? tune->tile_segs : 1, tune->tile_tz};
+            if (!valid_tile_shape(cfgs[0].dim, t)) {
+                set_error("bad tile shape: rows 4..32, segs 1..4, tz 1..rows, powers of two");
+                cudaStreamDestroy(b->st);
+                delete b;
+                return BP_ERR_ARG;
+            }
+            b->core.shape = t;
+        }
         b->core.ctas_per_sm = tune->ctas_per_sm;
         b->core.steps_per_sync = tune->steps_per_sync;
-        b->user_tuned = tune->ctas_per_sm > 0 && tune->steps_per_sync > 0;
+        b->user_tuned = tune->ctas_per_sm > 0 && tune->steps_per_sync > 0 && tune->tile_rows > 0;
     }
     for (int i = 0; i < nshots; i++) {
         auto sh = std::make_unique<Shot>();
@@ -236,6 +298,32 @@ int bp_batch_run(bp_batch* b, int nsteps) {
     return b->core.advance(nsteps);
 }
 
+int bp_batch_run_timed(bp_batch* b, int nsteps, float* ms) {
+    if (!b || nsteps < 0 || !ms) { set_error("bad arguments"); return BP_ERR_ARG; }
+    cudaSetDevice(b->core.device);
+    if (!b->core.tuned) {
+        int rc = bp_batch_autotune(b, nsteps);
+        if (rc) return rc;
+    }
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        set_error("cudaEventCreate failed");
+        return BP_ERR_CUDA;
+    }
+    cudaEventRecord(e0, b->st);
+    int rc = b->core.advance(nsteps);
+    cudaEventRecord(e1, b->st);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float t = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
+    *ms = t;
+    return BP_OK;
+}
+
 int bp_batch_sync(bp_batch* b) {
     if (!b) { set_error("null batch"); return BP_ERR_ARG; }
     cudaError_t e = cudaStreamSynchronize(b->st);
@@ -268,9 +356,23 @@ int bp_batch_get_traces(bp_batch* b, int shot, int comp, float* host, size_t n) 
 int bp_batch_get_tune(bp_batch* b, bp_tune* chosen) {
     if (!b || !chosen) { set_error("bad arguments"); return BP_ERR_ARG; }
     memset(chosen, 0, sizeof(*chosen));
-    chosen->tile_rows = tile_rows();
+    TileShape t = b->core.effective_shape();
+    if (b->core.dim == 3 && t.tz == 0) t.tz = default_tile_shape(3, b->core.prec).tz;
+    chosen->tile_rows = t.rows;
+    chosen->tile_segs = t.segs;
+    chosen->tile_tz = b->core.dim == 3 ? t.tz : 1;
     chosen->steps_per_sync = b->core.steps_per_sync;
     chosen->ctas_per_sm = b->core.ctas_per_sm;
+    return BP_OK;
+}
+
+int bp_batch_autotune(bp_batch* b, int budget_steps) {
+    if (!b || budget_steps < 0) { set_error("bad arguments"); return BP_ERR_ARG; }
+    cudaSetDevice(b->core.device);
+    if (b->user_tuned) return BP_OK;
+    int rc = b->core.autotune(budget_steps);
+    if (rc) return rc;
+    b->core.tuned = true;
     return BP_OK;
 }
 

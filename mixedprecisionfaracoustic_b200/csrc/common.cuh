@@ -56,7 +56,10 @@ struct ShotDesc {
     int nseg;                     // 128-cell x segments per row
     int nrows;                    // rows per shot: ny * nz (3D) or nz (2D)
     long long tile0;              // first tile index of this shot in the batch
-    int rows_per_tile;
+    // tile shape of the register kernels (TileShape): 2^tile_lr rows (3D:
+    // 2^(tile_lr - tile_ltz) y rows of 2^tile_ltz z planes) x 2^tile_ls
+    // 128-cell segments; nseg_t = tiles per row block along x
+    int tile_lr, tile_ls, tile_ltz, nseg_t;
     int nt;                       // trace length
     int src_idx_valid;
     long long src_idx;            // flat index of the source cell
@@ -169,6 +172,7 @@ __device__ __forceinline__ T ldv(const T* p) {
 struct PolF32 {
     using real = float;
     static constexpr int prec = BP_PREC_FP32;
+    static constexpr bool exact = false;      // reference rounding (PolF32R)
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
         float4 t = ldv<NC>(reinterpret_cast<const float4*>(static_cast<const float*>(p) + i));
@@ -204,6 +208,7 @@ struct PolF32 {
 struct PolF64 {
     using real = double;
     static constexpr int prec = BP_PREC_FP64;
+    static constexpr bool exact = false;
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
         const double2* q = reinterpret_cast<const double2*>(static_cast<const double*>(p) + i);
@@ -239,11 +244,24 @@ struct PolF64 {
     __device__ __forceinline__ static real dec1(raw1 t) { return t; }
 };
 
+// FP32 with the reference Float build's rounding where PolF32 rounds
+// differently (bp_config.rounding = BP_ROUND_REFERENCE): the division by H is
+// the IEEE quotient (PolF32: reciprocal plus one residual step, within one
+// ulp), and the CPML memory update psi e + b (e prev + d) adds b (e prev + d)
+// to the float product psi e with one rounding, which is what the reference's
+// double-promoted expression gives (Float/main.cu:130-158,252-285: float
+// psi e, the double product 0.5 fl(-DT d) (e prev + d), one rounding of the
+// double sum to float).  Same storage as PolF32.
+struct PolF32R : PolF32 {
+    static constexpr bool exact = true;
+};
+
 // COMP16: fp16 hi (8 bytes per 4 cells) + int8 lo (4 bytes per 4 cells).
 // A null lo pointer means "hi only" (used for fp16-only coefficient storage).
 struct PolC16 {
     using real = float;
     static constexpr int prec = BP_PREC_COMP16;
+    static constexpr bool exact = false;
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t* lo, cidx i, real (&v)[4]) {
         uint2 h = ldv<NC>(reinterpret_cast<const uint2*>(static_cast<const __half*>(p) + i));

@@ -2,12 +2,11 @@
 // device allocation.
 //
 // bp_rel_l2_device allocates its reduction scratch with cudaMalloc on every
-// call.  Some callers cannot allow that: code running while a CUDA stream is
-// being captured into a graph (cudaMalloc is not a stream operation and is
-// refused during capture in the strict modes), real-time loops that must not
-// stall on the allocator's implicit device synchronisation, and processes that
-// hand all device memory to their own pool up front.  This variant keeps its
-// scratch in a fixed array that lives in the library's device image instead.
+// call.  Some callers cannot allow that: real-time loops that must not stall
+// on the implicit device synchronisation cudaMalloc/cudaFree can bring, and
+// processes that hand all device memory to their own pool up front, where a
+// cudaMalloc fails.  This variant keeps its scratch in a fixed array that lives
+// in the library's device image instead.
 //
 // Scratch: one (sum of squared differences, sum of squared reference values)
 // partial pair per block, at most kMaxBlocks blocks, plus the final pair: about
@@ -16,11 +15,17 @@
 // kMaxBlocks * kPerBlock = 16,777,216; larger inputs are rejected with
 // BP_ERR_ARG.
 //
+// The call is synchronous: both kernels run on the legacy default stream and
+// the result comes back by a blocking cudaMemcpy, so the function returns once
+// the value is known.  Work still running on other streams (the library's own
+// streams are created non-blocking) is not ordered before it: the inputs must
+// be complete, so synchronise the stream that produces them first.
+//
 // Every call on a device shares that one array, which keeps the last call's
 // contents.  Nothing in it needs to start at zero: each call writes every
 // partial it reads and then the final pair.  Two calls whose kernels overlap
-// on the GPU (different streams, or different host threads without ordering)
-// race on the array and may return wrong results; serialise them.
+// on the GPU (calls from different host threads without ordering) race on the
+// array and may return wrong results; serialise them.
 //
 // The device address of the array is looked up with cudaGetSymbolAddress once
 // per device, by the first call made while that device is current; make that

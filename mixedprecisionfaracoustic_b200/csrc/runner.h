@@ -27,6 +27,8 @@ struct Runner {
     size_t d_err_bytes = 0;            // its block (from the arena cache)
     int variant = BP_KERNEL_AUTO;      // BP_KERNEL_*: which phase-kernel family runs
     bool post_in_t = false;            // every shot's receivers and source lie in cells the T phase visits
+    int rounding = BP_ROUND_FAST;      // FP32 BP_ROUND_REFERENCE: PolF32R register kernels only
+    bool multi_unit = false;           // the shots' tile shape has more units than a CTA has warps
 
     void configure(int prec_, int dim_, int order_, const ShotDesc* d, int n, long long tiles, long long tiles_s,
                    long long tiles_m, int maxrec, cudaStream_t s, int ctas_per_sm, int steps_per_graph) {
@@ -35,7 +37,7 @@ struct Runner {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        int ov = phase_occupancy(prec, dim, order, true), ot = phase_occupancy(prec, dim, order, false);
+        int ov = phase_occupancy(prec, dim, order, true, rounding), ot = phase_occupancy(prec, dim, order, false, rounding);
         if (ctas_per_sm > 0) { ov = ov < ctas_per_sm ? ov : ctas_per_sm; ot = ot < ctas_per_sm ? ot : ctas_per_sm; }
         long long gv = (long long)ov * sms, gt = (long long)ot * sms;
         grid_v = (int)(gv < tiles ? gv : (tiles > 0 ? tiles : 1));
@@ -52,9 +54,9 @@ struct Runner {
         reset_graph();
     }
     void select_kernels() {
-        const bool can_m = march_supported(prec, dim) && ntiles_m > 0;
+        const bool can_m = march_supported(prec, dim) && ntiles_m > 0 && rounding == BP_ROUND_FAST;
         march = can_m && (variant == BP_KERNEL_MARCH || (variant == BP_KERNEL_AUTO && march_default()));
-        const bool can = staged_supported(prec, dim) && ntiles_s > 0;
+        const bool can = staged_supported(prec, dim) && ntiles_s > 0 && rounding == BP_ROUND_FAST;
         staged = !march && can && (variant == BP_KERNEL_STAGED || (variant == BP_KERNEL_AUTO && staged_default()));
     }
     void reset_graph() {
@@ -83,7 +85,7 @@ struct Runner {
         if (march) return launch_phase_march(prec, order, v, d_shots, nshots, ntiles_m, k, st);
         if (staged) return launch_phase_staged(prec, order, v, d_shots, nshots, ntiles_s, k, grid_s, d_err, st);
         return launch_phase(prec, dim, order, v, d_shots, nshots, ntiles, k, v ? grid_v : grid_t, st,
-                            (!v && fused_post()) ? 1 : 0);
+                            (!v && fused_post()) ? 1 : 0, rounding, multi_unit);
     }
 
     // m steps issued directly (k = 0..m-1), then the step bases advance by m.

@@ -57,7 +57,7 @@ struct bp_server {
     int worker_error = 0;
 };
 
-// One batch per (dim, order, precision) class; each class has its own stream
+// One batch per (dim, order, precision, rounding) class; each class has its own stream
 // so the classes' launches overlap on the device.
 struct ClassBatch {
     BatchCore core;
@@ -69,7 +69,7 @@ struct ClassBatch {
 static void server_loop(bp_server* s) {
     cudaSetDevice(s->device);
     std::map<int, std::unique_ptr<ClassBatch>> classes;
-    auto klass = [](const bp_config& c) { return c.dim * 100 + c.order * 10 + c.precision; };
+    auto klass = [](const bp_config& c) { return c.rounding * 1000 + c.dim * 100 + c.order * 10 + c.precision; };
     for (;;) {
         std::vector<Request*> admit;
         size_t nrun = 0;
@@ -109,6 +109,7 @@ static void server_loop(bp_server* s) {
                 cudaStreamCreateWithFlags(&cb->st, cudaStreamNonBlocking);
                 cb->core.init(s->device, cb->st);
                 cb->core.dim = r->cfg.dim; cb->core.order = r->cfg.order; cb->core.prec = r->cfg.precision;
+                cb->core.rounding = r->cfg.rounding;
                 cb->core.steps_per_sync = s->sps;
             }
             const size_t n = r->medium.size() / 9;

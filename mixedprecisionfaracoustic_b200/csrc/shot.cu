@@ -7,6 +7,7 @@
 //   indices, trace and snapshot buffers, reduction scratch and the device copy
 //   of the shot descriptor.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -44,6 +45,11 @@ int validate_config(const bp_config* c) {
     if (c->dim != 2 && c->dim != 3) { set_error("dim must be 2 or 3"); return BP_ERR_ARG; }
     if (c->order != 2 && c->order != 4) { set_error("order must be 2 or 4"); return BP_ERR_ARG; }
     if (c->precision < BP_PREC_FP32 || c->precision > BP_PREC_FP64) { set_error("bad precision"); return BP_ERR_ARG; }
+    if (c->rounding != BP_ROUND_FAST && c->rounding != BP_ROUND_REFERENCE) { set_error("bad rounding"); return BP_ERR_ARG; }
+    if (c->rounding == BP_ROUND_REFERENCE && c->precision != BP_PREC_FP32) {
+        set_error("reference rounding applies to FP32 only");
+        return BP_ERR_ARG;
+    }
     if (c->nx < 1 || c->nz < 1 || (c->dim == 3 && c->ny < 1) || c->npml < 0) { set_error("bad grid size"); return BP_ERR_ARG; }
     const int hw = c->order / 2;
     const int nx = c->nx + 2 * c->npml, nz = c->nz + 2 * c->npml, ny = c->dim == 3 ? c->ny + 2 * c->npml : 1;
@@ -278,7 +284,6 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     S.nseg = (p.nx + seg_cells() - 1) / seg_cells();
     S.nrows = p.ny * p.nz;
     S.tile0 = 0;
-    S.rows_per_tile = tile_rows();
     S.tile0s = 0;
     S.nseg_s = (p.nx + staged_tile_width() - 1) / staged_tile_width();
     S.tile0m = 0;
@@ -454,6 +459,7 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
         e = cudaMemcpyAsync((void*)S.rec_row, row_start.data(), row_start.size() * 4, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && nurec > 0)
         e = cudaMemcpyAsync((void*)S.rec_xu, xu.data(), (size_t)nurec * 8, cudaMemcpyHostToDevice, st);
+    ntiles = apply_tile_shape(S, dim, c->precision, default_tile_shape(dim, c->precision));
     d_desc = (ShotDesc*)(A + p.o_desc);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_desc, &S, sizeof(ShotDesc), cudaMemcpyHostToDevice, st);
@@ -465,7 +471,6 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
 
     long long cx = p.nx - 2 * S.hw, cz = p.nz - 2 * S.hw, cy = dim == 3 ? p.ny - 2 * S.hw : 1;
     cells = cx * cy * cz;
-    ntiles = (long long)S.nseg * tile_row_blocks(dim, c->precision, S.ny, S.nz);
     ntiles_s = (long long)S.nseg_s * ((S.nrows + staged_tile_rows() - 1) / staged_tile_rows());
     ntiles_m = dim == 2 ? (long long)S.ncol_m * ((p.nz - 2 * S.hw + S.zseg_m - 1) / S.zseg_m) : 0;
     it_host = 0;
@@ -555,7 +560,21 @@ void free_cached(int device) {   // g_arena_mu held; device -1 = all devices
 // An arena of at least `bytes` on the current device: a cached one of up to
 // 1.25x that size, else a new allocation (after emptying this device's cache
 // if the first attempt fails).  *got is the block's real size.
+// Injected allocation failure (bp_debug_fail_allocation): the number of
+// arena requests left until the one that fails, 0 = none armed.
+static std::atomic<long long> g_fail_in{0};
+
+void arm_allocation_failure(long long nth) { g_fail_in.store(nth > 0 ? nth : 0); }
+
 cudaError_t arena_alloc(size_t bytes, void** ptr, size_t* got) {
+    // a request the test hook marks fails like an exhausted device, before it
+    // takes a cached block or calls cudaMalloc, so nothing is held
+    for (long long n = g_fail_in.load(); n > 0;) {
+        if (g_fail_in.compare_exchange_weak(n, n - 1)) {
+            if (n == 1) return cudaErrorMemoryAllocation;
+            break;
+        }
+    }
     int dev = 0;
     cudaGetDevice(&dev);
     {

@@ -14,8 +14,11 @@ namespace bpk {
 // launchers (step.cu, precompute.cu, reduce.cu)
 // post = 1: the T phase also records the receivers and injects the next source
 // sample (every receiver and the source lie in cells the T phase visits)
+// rounding = BP_ROUND_REFERENCE (FP32): the PolF32R instantiation; multi: the
+// tile shape has more (row, segment) units than a CTA has warps
 cudaError_t launch_phase(int prec, int dim, int order, bool vphase, const ShotDesc* d_shots, int nshots,
-                         long long ntiles, int k, int grid, cudaStream_t st, int post = 0);
+                         long long ntiles, int k, int grid, cudaStream_t st, int post = 0, int rounding = 0,
+                         bool multi = false);
 cudaError_t launch_post(int prec, const ShotDesc* d_shots, int nshots, int max_rec, int k, int do_record,
                         cudaStream_t st);
 cudaError_t launch_inject(int prec, const ShotDesc* d_shots, int nshots, int k, cudaStream_t st);
@@ -25,8 +28,17 @@ cudaError_t launch_snapshot(int prec, const ShotDesc* d_shots, int shot, int f, 
 cudaError_t launch_field_f64(int prec, const ShotDesc* d_shots, int f, double* out, cudaStream_t st);
 cudaError_t launch_coef(int prec, const ShotDesc* d_shots, int which, float* out, cudaStream_t st);
 int phase_threads();
-int tile_rows();
-long long tile_row_blocks(int dim, int prec, int ny, int nz);   // row blocks of the tile kernels per shot
+// Tile of the register kernels: `rows` rows (z rows in 2D; in 3D rows/tz y
+// rows of tz z planes) x `segs` 128-cell segments along x, taken by the 8 warps
+// of a CTA one (row, segment) unit at a time.  Powers of two: rows 4..32,
+// segs 1..4, tz 1..rows.  Every shape gives the same results.
+struct TileShape {
+    int rows = 8, segs = 1, tz = 0;    // tz = 0: the precision's default split
+};
+TileShape default_tile_shape(int dim, int prec);
+bool valid_tile_shape(int dim, const TileShape& t);
+// Writes the shape into the descriptor and returns the shot's tile count.
+long long apply_tile_shape(ShotDesc& S, int dim, int prec, TileShape t);
 int seg_cells();
 // TMA-staged 2D phase kernels (step_staged.cu)
 bool staged_supported(int prec, int dim);
@@ -35,7 +47,7 @@ int staged_tile_rows();
 int staged_tile_width();
 cudaError_t launch_phase_staged(int prec, int order, bool vphase, const ShotDesc* d, int nshots, long long ntiles,
                                 int k, int grid, int* err, cudaStream_t st);
-int phase_occupancy(int prec, int dim, int order, bool vphase);
+int phase_occupancy(int prec, int dim, int order, bool vphase, int rounding = 0);
 // register-window marching 2D phase kernels (step_march.cu)
 bool march_supported(int prec, int dim);
 bool march_default();            // whether BP_KERNEL_AUTO picks the marching kernels where supported
@@ -63,6 +75,7 @@ void set_error(const std::string& msg);
 cudaError_t arena_alloc(size_t bytes, void** ptr, size_t* got);
 void arena_release(void* ptr, size_t bytes);
 void release_cached_arenas(int device);   // -1: every device
+void arm_allocation_failure(long long nth);   // bp_debug_fail_allocation
 
 struct Shot {
     bp_config cfg{};
@@ -85,7 +98,7 @@ struct Shot {
     double* d_out = nullptr;           // 4 doubles
     long long cells = 0;               // updated cells per step
     int it_host = 0;                   // steps issued so far
-    long long ntiles = 0;              // tiles of the register kernels (128 x 8)
+    long long ntiles = 0;              // tiles of the register kernels (current TileShape)
     long long ntiles_s = 0;            // tiles of the TMA-staged 2D kernels (256 x staged_tile_rows)
     long long ntiles_m = 0;            // tasks of the marching 2D kernels (128 cells x zseg_m rows)
     bool post_in_t = false;            // receivers and source all in cells the T phase visits

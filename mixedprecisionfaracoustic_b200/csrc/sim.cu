@@ -97,6 +97,12 @@ const char* bp_error_string(int code) {
 }
 const char* bp_last_error(void) { return last_error_cstr(); }
 
+int bp_debug_fail_allocation(int nth) {
+    if (nth < 0) { set_error("nth must be >= 0"); return BP_ERR_ARG; }
+    arm_allocation_failure(nth);
+    return BP_OK;
+}
+
 int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out) {
     if (!out) { set_error("null output pointer"); return BP_ERR_ARG; }
     *out = nullptr;
@@ -137,6 +143,7 @@ int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out) {
     if (!rc && crc) { cudaStreamSynchronize(s->st); rc = crc; }
     if (rc) { s->shot.destroy(); cudaStreamDestroy(s->st); delete s; return rc; }
     s->run.post_in_t = s->shot.post_in_t;
+    s->run.rounding = cfg->rounding;
     s->run.configure(cfg->precision, cfg->dim, cfg->order, s->shot.d_desc, 1, s->shot.ntiles, s->shot.ntiles_s,
                      s->shot.ntiles_m, s->shot.nurec, s->st, 0, 32);
     *out = s;
@@ -220,6 +227,10 @@ int bp_set_kernel(bp_sim* s, int variant) {
     }
     if (variant == BP_KERNEL_MARCH && !march_supported(s->shot.cfg.precision, s->shot.cfg.dim)) {
         set_error("the marching kernels cover 2D FP32 and COMP16 only");
+        return BP_ERR_ARG;
+    }
+    if ((variant == BP_KERNEL_STAGED || variant == BP_KERNEL_MARCH) && s->shot.cfg.rounding != BP_ROUND_FAST) {
+        set_error("reference rounding runs the register tile kernels only");
         return BP_ERR_ARG;
     }
     SIM_CK(cudaStreamSynchronize(s->st));

@@ -14,8 +14,12 @@ __device__ __forceinline__ typename P::real deriv_div(typename P::real a, const 
     // step, q += (a - q H) * (1/H), with the exact fused residual a - q H,
     // matches the IEEE quotient a / H to within one ulp (equal in all but rare
     // near-tie cases) in 3 instructions instead of a full divide.
-    // FP64 divides; COMP16 (own arithmetic) multiplies by 1/H.
+    // FP64 divides; COMP16 (own arithmetic) multiplies by 1/H.  PolF32R takes
+    // the IEEE quotient like the reference; a zero dividend (the quiet grid
+    // ahead of the wavefront), which sends the divide routine down its slow
+    // path, gives the same signed zero as a product.
     if constexpr (P::prec == BP_PREC_FP64) return a / (typename P::real)S.hd;
+    else if constexpr (P::prec == BP_PREC_FP32 && P::exact) return a == 0.0f ? a * S.inv_h : __fdiv_rn(a, S.h);
     else if constexpr (P::prec == BP_PREC_FP32) {
         const float q = a * S.inv_h;
         return __fmaf_rn(__fmaf_rn(-q, S.h, a), S.inv_h, q);
@@ -91,11 +95,20 @@ __device__ __forceinline__ void scale4(R (&v)[4], R r) {
     for (int j = 0; j < 4; j++) v[j] = mulr(v[j], r);
 }
 
+// New ψ of one cell: ψ e + b (e prev + ∂).  EX (FP32 only): e prev + ∂ fused,
+// then added times b to the float product ψ e with one rounding, as the
+// reference's double-promoted expression rounds it (Float/main.cu:130-158).
+template <bool EX, class R>
+__device__ __forceinline__ R cpml_psi(R ps, R pv, R d, R bb, R ee) {
+    if constexpr (EX) return __fmaf_rn(bb, __fmaf_rn(ee, pv, d), __fmul_rn(ps, ee));
+    else return ps * ee + bb * (ee * pv + d);
+}
+
 // CPML memory update of one derivative slot for a 4-cell chunk
 // (Float/main.cu:130-158):  ψ = ψ e + b (e prev + ∂),  prev = ∂,  ∂ += ψ,
 // with b = -DT d / 2 precomputed.  The x axis has per-cell tables; the y and z
 // axes one value per chunk.  Old ψ/prev are multiplied by the state rescale r.
-template <bool RS, class R>
+template <bool RS, class R, bool EX = false>
 __device__ __forceinline__ void cpml_x(R (&d)[4], R* psi, R* prev, const R* b, const R* e, int x0, R r) {
     R ps[4], pv[4];
 #pragma unroll
@@ -106,7 +119,7 @@ __device__ __forceinline__ void cpml_x(R (&d)[4], R* psi, R* prev, const R* b, c
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         R ee = e[x0 + j], bb = b[x0 + j];
-        R np = ps[j] * ee + bb * (ee * pv[j] + d[j]);
+        R np = cpml_psi<EX>(ps[j], pv[j], d[j], bb, ee);
         ps[j] = np;
         pv[j] = d[j];
         d[j] = d[j] + np;
@@ -114,7 +127,7 @@ __device__ __forceinline__ void cpml_x(R (&d)[4], R* psi, R* prev, const R* b, c
 #pragma unroll
     for (int j = 0; j < 4; j++) { psi[j] = ps[j]; prev[j] = pv[j]; }
 }
-template <bool RS, class R>
+template <bool RS, class R, bool EX = false>
 __device__ __forceinline__ void cpml_s(R (&d)[4], R* psi, R* prev, R bb, R ee, R r) {
     R ps[4], pv[4];
 #pragma unroll
@@ -124,7 +137,7 @@ __device__ __forceinline__ void cpml_s(R (&d)[4], R* psi, R* prev, R bb, R ee, R
     }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-        R np = ps[j] * ee + bb * (ee * pv[j] + d[j]);
+        R np = cpml_psi<EX>(ps[j], pv[j], d[j], bb, ee);
         ps[j] = np;
         pv[j] = d[j];
         d[j] = d[j] + np;
@@ -157,7 +170,7 @@ struct PsiIO {
 
 // One derivative slot of one axis: memory variables k (ψ) and NS+k (prev) of
 // the (phase, axis) slab array; fwd selects the half-grid profile.
-template <int NS, bool RS, class R>
+template <int NS, bool RS, class R, bool EX = false>
 __device__ __forceinline__ void cpml_slot(R (&d)[4], void* base, long long cells, int k, cidx sidx,
                                           bool xaxis, int pos, int x0, const void* pb, const void* pe, R r) {
     R* ps = static_cast<R*>(base) + (long long)k * cells + sidx;
@@ -167,8 +180,8 @@ __device__ __forceinline__ void cpml_slot(R (&d)[4], void* base, long long cells
     PsiIO<R>::ld(pv, pvv);
     const R* b = static_cast<const R*>(pb);
     const R* e = static_cast<const R*>(pe);
-    if (xaxis) cpml_x<RS, R>(d, psv, pvv, b, e, x0, r);
-    else cpml_s<RS, R>(d, psv, pvv, b[pos], e[pos], r);
+    if (xaxis) cpml_x<RS, R, EX>(d, psv, pvv, b, e, x0, r);
+    else cpml_s<RS, R, EX>(d, psv, pvv, b[pos], e[pos], r);
     PsiIO<R>::st(ps, psv);
     PsiIO<R>::st(pv, pvv);
 }
@@ -243,30 +256,30 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y,
         if (si >= 0) {
             void* B = S.psiV[0];
             const long long n = S.slab_cells[0];
-            cpml_slot<NS, RS, R>(x1, B, n, 0, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            cpml_slot<NS, RS, R>(s1, B, n, 1, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            cpml_slot<NS, RS, R>(z2, B, n, 2, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            if constexpr (DIM == 3) cpml_slot<NS, RS, R>(y2, B, n, 3, si, true, x0, x0, S.pb[0], S.pe[0], r);
+            cpml_slot<NS, RS, R, P::exact>(x1, B, n, 0, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
+            cpml_slot<NS, RS, R, P::exact>(s1, B, n, 1, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
+            cpml_slot<NS, RS, R, P::exact>(z2, B, n, 2, si, true, x0, x0, S.pb[0], S.pe[0], r);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(y2, B, n, 3, si, true, x0, x0, S.pb[0], S.pe[0], r);
         }
         if constexpr (DIM == 3) {
             si = slab_index(S, 1, x0, y, z);
             if (si >= 0) {
                 void* B = S.psiV[1];
                 const long long n = S.slab_cells[1];
-                cpml_slot<NS, RS, R>(x2, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, RS, R>(y1, B, n, 1, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, RS, R>(s2, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, RS, R>(z3, B, n, 3, si, false, y, x0, S.pb[1], S.pe[1], r);
+                cpml_slot<NS, RS, R, P::exact>(x2, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
+                cpml_slot<NS, RS, R, P::exact>(y1, B, n, 1, si, false, y, x0, S.pb2[1], S.pe2[1], r);
+                cpml_slot<NS, RS, R, P::exact>(s2, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
+                cpml_slot<NS, RS, R, P::exact>(z3, B, n, 3, si, false, y, x0, S.pb[1], S.pe[1], r);
             }
         }
         si = slab_index(S, 2, x0, y, z);
         if (si >= 0) {
             void* B = S.psiV[2];
             const long long n = S.slab_cells[2];
-            cpml_slot<NS, RS, R>(x3, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, RS, R>(z1, B, n, 1, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            cpml_slot<NS, RS, R>(s3, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            if constexpr (DIM == 3) cpml_slot<NS, RS, R>(y3, B, n, 3, si, false, z, x0, S.pb[2], S.pe[2], r);
+            cpml_slot<NS, RS, R, P::exact>(x3, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
+            cpml_slot<NS, RS, R, P::exact>(z1, B, n, 1, si, false, z, x0, S.pb2[2], S.pe2[2], r);
+            cpml_slot<NS, RS, R, P::exact>(s3, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(y3, B, n, 3, si, false, z, x0, S.pb[2], S.pe[2], r);
         }
     }
 
@@ -385,30 +398,30 @@ __device__ __forceinline__ void t_tail(const ShotDesc& S, cidx c, int x0, int y,
         if (si >= 0) {
             void* B = S.psiT[0];
             const long long n = S.slab_cells[0];
-            cpml_slot<NS, RS, R>(uxx, B, n, 0, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            cpml_slot<NS, RS, R>(wx, B, n, 1, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            cpml_slot<NS, RS, R>(uzx, B, n, 2, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            if constexpr (DIM == 3) cpml_slot<NS, RS, R>(uyx, B, n, 3, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
+            cpml_slot<NS, RS, R, P::exact>(uxx, B, n, 0, si, true, x0, x0, S.pb[0], S.pe[0], r);
+            cpml_slot<NS, RS, R, P::exact>(wx, B, n, 1, si, true, x0, x0, S.pb[0], S.pe[0], r);
+            cpml_slot<NS, RS, R, P::exact>(uzx, B, n, 2, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(uyx, B, n, 3, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
         }
         if constexpr (DIM == 3) {
             si = slab_index(S, 1, x0, y, z);
             if (si >= 0) {
                 void* B = S.psiT[1];
                 const long long n = S.slab_cells[1];
-                cpml_slot<NS, RS, R>(uyy, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, RS, R>(wy, B, n, 1, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, RS, R>(uxy, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, RS, R>(uzy, B, n, 3, si, false, y, x0, S.pb2[1], S.pe2[1], r);
+                cpml_slot<NS, RS, R, P::exact>(uyy, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
+                cpml_slot<NS, RS, R, P::exact>(wy, B, n, 1, si, false, y, x0, S.pb[1], S.pe[1], r);
+                cpml_slot<NS, RS, R, P::exact>(uxy, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
+                cpml_slot<NS, RS, R, P::exact>(uzy, B, n, 3, si, false, y, x0, S.pb2[1], S.pe2[1], r);
             }
         }
         si = slab_index(S, 2, x0, y, z);
         if (si >= 0) {
             void* B = S.psiT[2];
             const long long n = S.slab_cells[2];
-            cpml_slot<NS, RS, R>(uzz, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, RS, R>(wz, B, n, 1, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, RS, R>(uxz, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            if constexpr (DIM == 3) cpml_slot<NS, RS, R>(uyz, B, n, 3, si, false, z, x0, S.pb2[2], S.pe2[2], r);
+            cpml_slot<NS, RS, R, P::exact>(uzz, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
+            cpml_slot<NS, RS, R, P::exact>(wz, B, n, 1, si, false, z, x0, S.pb[2], S.pe[2], r);
+            cpml_slot<NS, RS, R, P::exact>(uxz, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(uyz, B, n, 3, si, false, z, x0, S.pb2[2], S.pe2[2], r);
         }
     }
 

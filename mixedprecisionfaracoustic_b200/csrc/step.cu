@@ -15,6 +15,7 @@
 // Neighbour rows (y, z) are re-read through L1/L2; DRAM sees each array once
 // per phase.  The CPML memory variables exist on the slabs only; a chunk
 // touches them only when it lies in a slab of that axis.
+#include "shot.h"
 #include "stencil.cuh"
 
 namespace bpk {
@@ -353,13 +354,13 @@ __device__ __forceinline__ void mask0(R (&d)[4], unsigned mask) {
 }
 // CPML of one derivative on the slab of `axis` (slot k, half-grid profile if
 // half); nothing outside that slab.  Slabs hold 3 slots per phase in 2D, 4 in 3D.
-template <int DIM, bool RS, class R>
+template <int DIM, bool RS, class R, bool EX = false>
 __device__ __forceinline__ void cpml_g(const ShotDesc& S, void* const (&psi)[3], int axis, int k, bool half,
                                        cidx si, int x0, int y, int z, R (&d)[4], R r) {
     if (si < 0) return;
     const void* pb = half ? S.pb2[axis] : S.pb[axis];
     const void* pe = half ? S.pe2[axis] : S.pe[axis];
-    cpml_slot<DIM == 3 ? 4 : 3, RS, R>(d, psi[axis], S.slab_cells[axis], k, si, axis == 0,
+    cpml_slot<DIM == 3 ? 4 : 3, RS, R, EX>(d, psi[axis], S.slab_cells[axis], k, si, axis == 0,
                                         axis == 0 ? x0 : (axis == 1 ? y : z), x0, pb, pe, r);
 }
 
@@ -399,20 +400,20 @@ __device__ __forceinline__ void v_comp(const ShotDesc& S, cidx c, cidx row, int 
     const cidx s0 = slab_index(S, 0, x0, y, z), s2 = slab_index(S, 2, x0, y, z);
     const cidx s1 = DIM == 3 ? slab_index(S, 1, x0, y, z) : -1;
     if constexpr (AX == 0) {
-        cpml_g<DIM, RS>(S, psi, 0, 0, true, s0, x0, y, z, dx, r);
-        cpml_g<DIM, RS>(S, psi, 0, 1, true, s0, x0, y, z, dp, r);
-        if constexpr (DIM == 3) cpml_g<DIM, RS>(S, psi, 1, 0, false, s1, x0, y, z, dy, r);
-        cpml_g<DIM, RS>(S, psi, 2, 0, false, s2, x0, y, z, dz, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 0, 0, true, s0, x0, y, z, dx, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 0, 1, true, s0, x0, y, z, dp, r);
+        if constexpr (DIM == 3) cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 1, 0, false, s1, x0, y, z, dy, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 2, 0, false, s2, x0, y, z, dz, r);
     } else if constexpr (AX == 1) {
-        cpml_g<DIM, RS>(S, psi, 0, 3, false, s0, x0, y, z, dx, r);
-        cpml_g<DIM, RS>(S, psi, 1, 1, true, s1, x0, y, z, dy, r);
-        cpml_g<DIM, RS>(S, psi, 1, 2, true, s1, x0, y, z, dp, r);
-        cpml_g<DIM, RS>(S, psi, 2, 3, false, s2, x0, y, z, dz, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 0, 3, false, s0, x0, y, z, dx, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 1, 1, true, s1, x0, y, z, dy, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 1, 2, true, s1, x0, y, z, dp, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 2, 3, false, s2, x0, y, z, dz, r);
     } else {
-        cpml_g<DIM, RS>(S, psi, 0, 2, false, s0, x0, y, z, dx, r);
-        if constexpr (DIM == 3) cpml_g<DIM, RS>(S, psi, 1, 3, false, s1, x0, y, z, dy, r);
-        cpml_g<DIM, RS>(S, psi, 2, 1, true, s2, x0, y, z, dz, r);
-        cpml_g<DIM, RS>(S, psi, 2, 2, true, s2, x0, y, z, dp, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 0, 2, false, s0, x0, y, z, dx, r);
+        if constexpr (DIM == 3) cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 1, 3, false, s1, x0, y, z, dy, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 2, 1, true, s2, x0, y, z, dz, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 2, 2, true, s2, x0, y, z, dp, r);
     }
     // the divergence in v_tail's summation order: x1 (+x2) +x3, y1+y2+y3, z1+z2 (+z3)
     R sum[4];
@@ -504,14 +505,14 @@ __device__ __forceinline__ void t_shear(const ShotDesc& S, cidx c, cidx row, int
     }
     mask0(a, mask); mask0(b, mask);
     if constexpr (SH == 0) {
-        cpml_g<DIM, RS>(S, psi, 0, 3, true, slab_index(S, 0, x0, y, z), x0, y, z, b, r);
-        cpml_g<DIM, RS>(S, psi, 1, 2, true, slab_index(S, 1, x0, y, z), x0, y, z, a, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 0, 3, true, slab_index(S, 0, x0, y, z), x0, y, z, b, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 1, 2, true, slab_index(S, 1, x0, y, z), x0, y, z, a, r);
     } else if constexpr (SH == 1) {
-        cpml_g<DIM, RS>(S, psi, 1, 3, true, slab_index(S, 1, x0, y, z), x0, y, z, b, r);
-        cpml_g<DIM, RS>(S, psi, 2, 3, true, slab_index(S, 2, x0, y, z), x0, y, z, a, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 1, 3, true, slab_index(S, 1, x0, y, z), x0, y, z, b, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 2, 3, true, slab_index(S, 2, x0, y, z), x0, y, z, a, r);
     } else {
-        cpml_g<DIM, RS>(S, psi, 0, 2, true, slab_index(S, 0, x0, y, z), x0, y, z, b, r);
-        cpml_g<DIM, RS>(S, psi, 2, 2, true, slab_index(S, 2, x0, y, z), x0, y, z, a, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 0, 2, true, slab_index(S, 0, x0, y, z), x0, y, z, b, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 2, 2, true, slab_index(S, 2, x0, y, z), x0, y, z, a, r);
     }
     constexpr int f = SH == 0 ? BP_F_TXY : SH == 1 ? BP_F_TYZ : BP_F_TXZ;
     constexpr int cm = SH == 0 ? TC_MUXY : SH == 1 ? TC_MUYZ : TC_MUXZ;
@@ -555,16 +556,16 @@ __device__ __forceinline__ void t_chunk_g(const ShotDesc& S, int x0, int y, int 
     if constexpr (DIM == 3) { mask0(uyy, mask); mask0(wy, mask); }
     {
         const cidx s0 = slab_index(S, 0, x0, y, z);
-        cpml_g<DIM, RS>(S, psi, 0, 0, false, s0, x0, y, z, uxx, r);
-        cpml_g<DIM, RS>(S, psi, 0, 1, false, s0, x0, y, z, wx, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 0, 0, false, s0, x0, y, z, uxx, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 0, 1, false, s0, x0, y, z, wx, r);
         if constexpr (DIM == 3) {
             const cidx s1 = slab_index(S, 1, x0, y, z);
-            cpml_g<DIM, RS>(S, psi, 1, 0, false, s1, x0, y, z, uyy, r);
-            cpml_g<DIM, RS>(S, psi, 1, 1, false, s1, x0, y, z, wy, r);
+            cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 1, 0, false, s1, x0, y, z, uyy, r);
+            cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 1, 1, false, s1, x0, y, z, wy, r);
         }
         const cidx s2 = slab_index(S, 2, x0, y, z);
-        cpml_g<DIM, RS>(S, psi, 2, 0, false, s2, x0, y, z, uzz, r);
-        cpml_g<DIM, RS>(S, psi, 2, 1, false, s2, x0, y, z, wz, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 2, 0, false, s2, x0, y, z, uzz, r);
+        cpml_g<DIM, RS, typename P::real, P::exact>(S, psi, 2, 1, false, s2, x0, y, z, wz, r);
     }
     R cC[4], cM[4], cH[4], cH2[4], o[4], n[4];
     const R dt = S.dtr<R>();
@@ -641,7 +642,7 @@ __device__ __forceinline__ void post_chunk(const ShotDesc& S, int it, cidx c, in
 // post (T phase only): each chunk also records the receivers in its cells and,
 // if it holds the source cell, injects the next source sample, in place of the
 // post-step kernel k_post.
-template <int DIM, int ORD, class P, bool VPHASE>
+template <int DIM, int ORD, class P, bool VPHASE, bool MU>
 __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHASE>())) k_phase(const ShotDesc* __restrict__ shots, int nshots,
                                                      long long ntiles, int k, int post) {
     using R = typename P::real;
@@ -673,64 +674,81 @@ __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHAS
             }
         }
         const ShotDesc& S = sdesc;
-        int seg, row;
+        int rb, sb;                           // row block and segment block of the tile
         if constexpr (step_once_per_shot<P>()) {
             if (!live) continue;
             const unsigned lt = (unsigned)(t - S.tile0);      // tiles of one shot < 2^32
-            const unsigned rb = lt / (unsigned)S.nseg;
-            seg = (int)(lt - rb * (unsigned)S.nseg);
-            row = (int)rb * kWarps + warp;
+            const unsigned q = lt / (unsigned)S.nseg_t;
+            rb = (int)q;
+            sb = (int)(lt - q * (unsigned)S.nseg_t);
         } else {
             const int it = *S.step_base + k;
             if (S.done || it >= S.nt) continue;
             it_cur = it;
             if constexpr (P::prec == BP_PREC_COMP16) r = S.rtab[it];
             const long long lt = t - S.tile0;
-            seg = (int)(lt % S.nseg);
-            row = (int)(lt / S.nseg) * kWarps + warp;
+            rb = (int)(lt / S.nseg_t);
+            sb = (int)(lt % S.nseg_t);
         }
-        int y, z;
-        if constexpr (DIM == 3) {
-            constexpr int TZ = tile_tz(P::prec), TY = kWarps / TZ;
-            const int rb = row / kWarps, nyb = (S.ny + TY - 1) / TY;
-            const int zb = rb / nyb, yb = rb - zb * nyb;
-            y = yb * TY + warp % TY;
-            z = zb * TZ + warp / TY;
-            if (y >= S.ny || z >= S.nz) continue;
-        } else {
-            if (row >= S.nrows) continue;
-            y = 0;
-            z = row;
-        }
-        const int hw = ORD / 2;
-        if (z < hw || z >= S.nz - hw) continue;
-        if (DIM == 3 && (y < hw || y >= S.ny - hw)) continue;
-        const int x0 = seg * kSegCells + lane * 4;
-        if (x0 >= S.nx - hw || x0 + 3 < hw) continue;
-        unsigned mask = 0;
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-            if (x0 + j >= hw && x0 + j < S.nx - hw) mask |= 1u << j;
-        // COMP16: the rescale products only on the steps whose factor is not
-        // exactly 1 (a uniform branch; the products are never fused, so both
-        // forms give the same bits when r == 1)
-        if constexpr (grouped<DIM, P, VPHASE>()) {
-            if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
-                if constexpr (VPHASE) v_chunk_g<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
-                else t_chunk_g<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+        // the tile's (row, segment) units, warp w taking units w, w + 8, ...;
+        // consecutive warps take consecutive rows
+        const int lr = S.tile_lr, units = 1 << (lr + S.tile_ls);
+        auto unit = [&](int u) {
+            const int ri = u & ((1 << lr) - 1);
+            const int seg = (sb << S.tile_ls) + (u >> lr);
+            if (seg >= S.nseg) return;
+            int y, z;
+            if constexpr (DIM == 3) {
+                const int ltz = S.tile_ltz, lty = lr - ltz;
+                const int nyb = (S.ny + (1 << lty) - 1) >> lty;
+                const int zb = rb / nyb, yb = rb - zb * nyb;
+                y = (yb << lty) + (ri & ((1 << lty) - 1));
+                z = (zb << ltz) + (ri >> lty);
+                if (y >= S.ny || z >= S.nz) return;
             } else {
-                if constexpr (VPHASE) v_chunk_g<DIM, ORD, P, false>(S, x0, y, z, r, mask);
-                else t_chunk_g<DIM, ORD, P, false>(S, x0, y, z, r, mask);
+                const int row = (rb << lr) + ri;
+                if (row >= S.nrows) return;
+                y = 0;
+                z = row;
             }
-        } else if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
-            if constexpr (VPHASE) v_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
-            else t_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+            const int hw = ORD / 2;
+            if (z < hw || z >= S.nz - hw) return;
+            if (DIM == 3 && (y < hw || y >= S.ny - hw)) return;
+            const int x0 = seg * kSegCells + lane * 4;
+            if (x0 >= S.nx - hw || x0 + 3 < hw) return;
+            unsigned mask = 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (x0 + j >= hw && x0 + j < S.nx - hw) mask |= 1u << j;
+            // COMP16: the rescale products only on the steps whose factor is not
+            // exactly 1 (a uniform branch; the products are never fused, so both
+            // forms give the same bits when r == 1)
+            if constexpr (grouped<DIM, P, VPHASE>()) {
+                if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
+                    if constexpr (VPHASE) v_chunk_g<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+                    else t_chunk_g<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+                } else {
+                    if constexpr (VPHASE) v_chunk_g<DIM, ORD, P, false>(S, x0, y, z, r, mask);
+                    else t_chunk_g<DIM, ORD, P, false>(S, x0, y, z, r, mask);
+                }
+            } else if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
+                if constexpr (VPHASE) v_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+                else t_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+            } else {
+                if constexpr (VPHASE) v_chunk<DIM, ORD, P, false>(S, x0, y, z, r, mask);
+                else t_chunk<DIM, ORD, P, false>(S, x0, y, z, r, mask);
+            }
+            if constexpr (!VPHASE)
+                if (post) post_chunk<DIM, P>(S, it_cur, x0 + y * (cidx)S.pitch + z * (cidx)S.plane, x0, y, z);
+        };
+        // MU: tiles of more units than warps (16-row or 8 x 2 tiles); the
+        // one-unit form keeps no loop state live across the chunk code, which
+        // costs the 2D FP32 V phase its spill-free 80 registers otherwise
+        if constexpr (MU) {
+            for (int u = warp; u < units; u += kWarps) unit(u);
         } else {
-            if constexpr (VPHASE) v_chunk<DIM, ORD, P, false>(S, x0, y, z, r, mask);
-            else t_chunk<DIM, ORD, P, false>(S, x0, y, z, r, mask);
+            if (warp < units) unit(warp);
         }
-        if constexpr (!VPHASE)
-            if (post) post_chunk<DIM, P>(S, it_cur, x0 + y * (cidx)S.pitch + z * (cidx)S.plane, x0, y, z);
     }
 }
 
@@ -922,12 +940,17 @@ __global__ void k_coef(const ShotDesc* __restrict__ shots, int which, float* out
 template <class P>
 struct Launch {
     static cudaError_t phase(int dim, int order, bool v, const ShotDesc* d_shots, int nshots, long long ntiles,
-                             int k, int grid, cudaStream_t st, int post) {
-#define BPK_LAUNCH(D, O)                                                                              \
-    if (dim == D && order == O) {                                                                     \
-        if (v) k_phase<D, O, P, true><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, 0);      \
-        else k_phase<D, O, P, false><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, post);    \
-        return cudaGetLastError();                                                                    \
+                             int k, int grid, cudaStream_t st, int post, bool multi) {
+#define BPK_LAUNCH(D, O)                                                                                        \
+    if (dim == D && order == O) {                                                                               \
+        if (multi) {                                                                                            \
+            if (v) k_phase<D, O, P, true, true><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, 0);      \
+            else k_phase<D, O, P, false, true><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, post);    \
+        } else {                                                                                                \
+            if (v) k_phase<D, O, P, true, false><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, 0);     \
+            else k_phase<D, O, P, false, false><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, post);   \
+        }                                                                                                       \
+        return cudaGetLastError();                                                                              \
     }
         BPK_LAUNCH(2, 2) BPK_LAUNCH(2, 4) BPK_LAUNCH(3, 2) BPK_LAUNCH(3, 4)
 #undef BPK_LAUNCH
@@ -940,10 +963,14 @@ struct Launch {
 // C++ entry points used by the host code (sim.cu, batch.cu).
 namespace bpk {
 cudaError_t launch_phase(int prec, int dim, int order, bool vphase, const ShotDesc* d_shots, int nshots,
-                         long long ntiles, int k, int grid, cudaStream_t st, int post) {
-    if (prec == BP_PREC_FP32) return Launch<PolF32>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post);
-    if (prec == BP_PREC_COMP16) return Launch<PolC16>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post);
-    return Launch<PolF64>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post);
+                         long long ntiles, int k, int grid, cudaStream_t st, int post, int rounding, bool multi) {
+    if (prec == BP_PREC_FP32 && rounding == BP_ROUND_REFERENCE)
+        return Launch<PolF32R>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
+    if (prec == BP_PREC_FP32)
+        return Launch<PolF32>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
+    if (prec == BP_PREC_COMP16)
+        return Launch<PolC16>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
+    return Launch<PolF64>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
 }
 
 cudaError_t launch_post(int prec, const ShotDesc* d_shots, int nshots, int max_rec, int k, int do_record,
@@ -983,13 +1010,15 @@ cudaError_t launch_field_f64(int prec, const ShotDesc* d_shots, int f, double* o
     return cudaGetLastError();
 }
 
-int phase_occupancy(int prec, int dim, int order, bool vphase) {
+int phase_occupancy(int prec, int dim, int order, bool vphase, int rounding) {
     int n = 0;
     const void* fn = nullptr;
 #define BPK_FN(PP, D, O)                                                                   \
     if (dim == D && order == O)                                                            \
-        fn = vphase ? (const void*)k_phase<D, O, PP, true> : (const void*)k_phase<D, O, PP, false>;
-    if (prec == BP_PREC_FP32) { BPK_FN(PolF32, 2, 2) BPK_FN(PolF32, 2, 4) BPK_FN(PolF32, 3, 2) BPK_FN(PolF32, 3, 4) }
+        fn = vphase ? (const void*)k_phase<D, O, PP, true, false> : (const void*)k_phase<D, O, PP, false, false>;
+    if (prec == BP_PREC_FP32 && rounding == BP_ROUND_REFERENCE) {
+        BPK_FN(PolF32R, 2, 2) BPK_FN(PolF32R, 2, 4) BPK_FN(PolF32R, 3, 2) BPK_FN(PolF32R, 3, 4)
+    } else if (prec == BP_PREC_FP32) { BPK_FN(PolF32, 2, 2) BPK_FN(PolF32, 2, 4) BPK_FN(PolF32, 3, 2) BPK_FN(PolF32, 3, 4) }
     else if (prec == BP_PREC_COMP16) { BPK_FN(PolC16, 2, 2) BPK_FN(PolC16, 2, 4) BPK_FN(PolC16, 3, 2) BPK_FN(PolC16, 3, 4) }
     else { BPK_FN(PolF64, 2, 2) BPK_FN(PolF64, 2, 4) BPK_FN(PolF64, 3, 2) BPK_FN(PolF64, 3, 4) }
 #undef BPK_FN
@@ -1005,13 +1034,43 @@ cudaError_t launch_coef(int prec, const ShotDesc* d_shots, int which, float* out
 }
 
 int phase_threads() { return kThreads; }
-int tile_rows() { return kWarps; }
-long long tile_row_blocks(int dim, int prec, int ny, int nz) {
+
+static int ilog2(int v) {
+    int l = 0;
+    while ((1 << (l + 1)) <= v) l++;
+    return l;
+}
+static bool pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+
+TileShape default_tile_shape(int dim, int prec) {
+    TileShape t;
+    t.rows = kWarps;
+    t.segs = 1;
+    t.tz = dim == 3 ? tile_tz(prec) : 1;
+    return t;
+}
+
+bool valid_tile_shape(int dim, const TileShape& t) {
+    if (!pow2(t.rows) || t.rows < 4 || t.rows > 32 || !pow2(t.segs) || t.segs > 4) return false;
+    if (dim == 3 && t.tz != 0 && (!pow2(t.tz) || t.tz > t.rows)) return false;
+    return true;
+}
+
+long long apply_tile_shape(ShotDesc& S, int dim, int prec, TileShape t) {
+    if (dim == 3 && t.tz == 0) t.tz = tile_tz(prec) < t.rows ? tile_tz(prec) : t.rows;
+    if (dim == 2) t.tz = 1;
+    S.tile_lr = ilog2(t.rows);
+    S.tile_ls = ilog2(t.segs);
+    S.tile_ltz = ilog2(t.tz);
+    S.nseg_t = (S.nseg + t.segs - 1) / t.segs;
+    long long blocks;
     if (dim == 3) {
-        const int tz = tile_tz(prec), ty = kWarps / tz;
-        return (long long)((ny + ty - 1) / ty) * ((nz + tz - 1) / tz);
+        const int ty = t.rows / t.tz;
+        blocks = (long long)((S.ny + ty - 1) / ty) * ((S.nz + t.tz - 1) / t.tz);
+    } else {
+        blocks = (S.nrows + t.rows - 1) / t.rows;
     }
-    return (nz + kWarps - 1) / kWarps;
+    return blocks * S.nseg_t;
 }
 int seg_cells() { return kSegCells; }
 }  // namespace bpk

@@ -66,10 +66,28 @@ def uniform_medium(shape: tuple, coef: dict) -> Medium:
     return Medium({k: np.full(shape, coef[k], dtype=np.float32) for k in MEDIUM_KEYS})
 
 
-def c0_coefficients() -> dict:
+def biot_from_moduli_host(Ks, Kb, mu, Kf, rhos, rhof, phi, tort, eta, kappa, m_shape=8.0) -> dict:
+    """The nine Biot coefficients of one material, in Python double arithmetic:
+    the formation branch of create_model (Float/main.cu:1635-1650), the same
+    operations in the same order as bp_biot_from_moduli, so the values are
+    bit-identical to the library's.  For callers that must not load the CUDA
+    library (the CPU reference arm of the benchmark)."""
+    alpha = 1 - Kb / Ks
+    M = Kf * Ks / (phi * Ks + (alpha - phi) * Kf)
+    H = alpha * alpha * M + Kb + mu * 4.0 / 3.0
+    vals = ((1 - phi) * rhos + phi * rhof, rhof, M, alpha * M, H, H - 2 * mu, mu, eta / kappa,
+            (1 + 2 / m_shape) * tort * rhof / phi)
+    return dict(zip(MEDIUM_KEYS, (float(v) for v in vals)))
+
+
+def _builder(host: bool):
+    return biot_from_moduli_host if host else biot_from_moduli
+
+
+def c0_coefficients(host: bool = False) -> dict:
     p = C0
-    return biot_from_moduli(p["Ks"], p["Kb"], p["mu"], p["Kf"], p["rhos"], p["rhof"], p["phi"], p["tort"],
-                            p["eta"], p["kappa"], p["m_shape"])
+    return _builder(host)(p["Ks"], p["Kb"], p["mu"], p["Kf"], p["rhos"], p["rhof"], p["phi"], p["tort"],
+                          p["eta"], p["kappa"], p["m_shape"])
 
 
 def _vmax(coefs: list) -> float:
@@ -102,8 +120,9 @@ def config0(precision: str = "fp32", order: int = 4, n: int = 160, npml: int = 2
     return cfg, uniform_medium((n, n, n), co)
 
 
-def layered_coefficients(seed: int, nlayers: int = 6):
-    """Per-layer Biot coefficients and thicknesses (cells) of the c1 layered model."""
+def layered_coefficients(seed: int, nlayers: int = 6, host: bool = False):
+    """Per-layer Biot coefficients and thicknesses (cells) of the c1 layered model
+    (host=True: formed without the CUDA library, bit-identical values)."""
     rng = np.random.default_rng(seed)
     thick = rng.integers(200, 501, size=nlayers)
     phi = rng.uniform(0.1, 0.35, nlayers)
@@ -111,14 +130,15 @@ def layered_coefficients(seed: int, nlayers: int = 6):
     kb = rng.uniform(5e9, 20e9, nlayers)
     mu = rng.uniform(3e9, 12e9, nlayers)
     p = C0
-    coefs = [biot_from_moduli(p["Ks"], float(kb[i]), float(mu[i]), p["Kf"], p["rhos"], p["rhof"], float(phi[i]),
-                              p["tort"], p["eta"], float(kappa[i]), p["m_shape"]) for i in range(nlayers)]
+    build = _builder(host)
+    coefs = [build(p["Ks"], float(kb[i]), float(mu[i]), p["Kf"], p["rhos"], p["rhof"], float(phi[i]),
+                   p["tort"], p["eta"], float(kappa[i]), p["m_shape"]) for i in range(nlayers)]
     return coefs, thick
 
 
-def layered_medium(nx: int, nz: int, seed: int, depth_scale: float = 1.0) -> tuple:
+def layered_medium(nx: int, nz: int, seed: int, depth_scale: float = 1.0, host: bool = False) -> tuple:
     """2D layered medium (nz, nx); layer thicknesses are scaled by depth_scale."""
-    coefs, thick = layered_coefficients(seed)
+    coefs, thick = layered_coefficients(seed, host=host)
     bounds = np.cumsum(np.maximum(1, np.round(thick * depth_scale).astype(int)))
     z = np.arange(nz)
     layer = np.searchsorted(bounds, z, side="right")
@@ -131,10 +151,11 @@ def layered_medium(nx: int, nz: int, seed: int, depth_scale: float = 1.0) -> tup
 
 
 def config1(precision: str = "fp32", seed: int = 1, nx: int = 4000, nz: int = 2000, nt: int = 8000,
-            npml: int = 20, order: int = 2, nrec: int = 2000):
-    """c1: 2D x-z layered model (scaled by nx, nz for tests)."""
+            npml: int = 20, order: int = 2, nrec: int = 2000, host: bool = False):
+    """c1: 2D x-z layered model (scaled by nx, nz for tests).  host=True forms
+    the medium without loading the CUDA library (same values)."""
     scale = nz / 2000.0
-    med, vmax = layered_medium(nx, nz, seed, depth_scale=scale)
+    med, vmax = layered_medium(nx, nz, seed, depth_scale=scale, host=host)
     sx = npml + int(round(2000 * nx / 4000.0))
     sz = npml + max(1, int(round(10 * scale)))
     rz = npml + max(1, int(round(10 * scale)))

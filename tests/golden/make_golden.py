@@ -1,7 +1,7 @@
 """Regenerates tests/golden/float_snapshots.npz from the reference's shipped
 golden snapshots (Float/*.dat: 192 x 192 y-mid slices written with "%e ").
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py <reference checkout>
 
 The reference project is read here, in the build container; the GPU box and
 the tests only read the committed .npz.
@@ -33,4 +33,6 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference checkout holding Float/*.dat>")
+    main(Path(sys.argv[1]))

@@ -106,3 +106,81 @@ def test_sharded_server_on_the_visible_devices():
         srv.release(gid)
     assert all(v == 0 for v in srv.outstanding.values())
     srv.close()
+
+
+SHAPES_2D = [(8, 1), (4, 2), (16, 1), (8, 2), (4, 1), (32, 1), (4, 4)]
+SHAPES_3D = [(8, 1, 1), (8, 1, 2), (8, 1, 4), (8, 1, 8), (16, 1, 4), (16, 1, 8), (4, 2, 2), (4, 1, 4)]
+
+
+def _shots_3d(prec, n=2, nt=90):
+    from mixedprecisionfaracoustic_b200.presets import c0_coefficients, uniform_medium
+    from mixedprecisionfaracoustic_b200.biot import ShotConfig
+    from mixedprecisionfaracoustic_b200 import _abi
+    out = []
+    for i, e in enumerate((22, 27)[:n]):
+        npml = 6
+        nxe = e + 2 * npml
+        c = nxe // 2
+        cfg = ShotConfig(dim=3, nx=e, ny=e + 3, nz=e - 2, npml=npml, order=2 + 2 * i, precision=prec, nt=nt,
+                         dx=5.0, dt=4e-4, f0=30.0, pml_v0=3300.0, pml_r=1e-6, src=(c, c, c - 2),
+                         src_mask=_abi.SRC_TAU | _abi.SRC_P, rec_x=list(range(npml, npml + e)),
+                         rec_y=[c] * e, rec_z=[npml + 2] * e)
+        out.append((cfg, uniform_medium((e - 2, e + 3, e), c0_coefficients())))
+    return out
+
+
+@pytest.mark.parametrize("prec", ["fp32", "comp16"])
+def test_every_tile_shape_gives_the_single_shot_results_2d(prec):
+    """The autotuner's tile shapes only change which warp takes which 4-cell
+    chunk: every shape gives bit-identical seismograms to the single runs."""
+    shots = config3_shots(seed=11, nshots=3, nt=120, precision=prec, scale=0.07)
+    singles = [alone(c, m) for c, m in shots]
+    for shape in SHAPES_2D:
+        b = Batch([c for c, _ in shots], [m for _, m in shots], steps_per_sync=16, ctas_per_sm=2, tile=shape)
+        b.run(120)
+        b.sync()
+        t = b.tune()
+        assert (t["tile_rows"], t["tile_segs"]) == shape
+        for i, (tx, tp) in enumerate(singles):
+            assert np.array_equal(b.traces(i, "txx"), tx), (shape, i)
+            assert np.array_equal(b.traces(i, "p"), tp), (shape, i)
+        b.close()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "comp16"])
+def test_every_tile_shape_gives_the_single_shot_results_3d(prec):
+    for order_shots in ([s] for s in _shots_3d(prec)):       # a batch holds one order
+        singles = [alone(c, m) for c, m in order_shots]
+        for shape in SHAPES_3D:
+            b = Batch([c for c, _ in order_shots], [m for _, m in order_shots], steps_per_sync=16, ctas_per_sm=2,
+                      tile=shape)
+            b.run(90)
+            b.sync()
+            t = b.tune()
+            assert (t["tile_rows"], t["tile_segs"], t["tile_tz"]) == shape
+            for i, (tx, tp) in enumerate(singles):
+                assert np.array_equal(b.traces(i, "txx"), tx), (shape, i)
+                assert np.array_equal(b.traces(i, "p"), tp), (shape, i)
+            b.close()
+
+
+def test_autotune_picks_a_shape_and_keeps_results():
+    shots = config3_shots(seed=12, nshots=4, nt=600, precision="fp32", scale=0.1)
+    singles = [alone(c, m) for c, m in shots]
+    b = Batch([c for c, _ in shots], [m for _, m in shots])
+    t = b.autotune(560)
+    assert t["tile_rows"] in (4, 8, 16, 32) and t["tile_segs"] in (1, 2, 4) and t["steps_per_sync"] > 0
+    b.run(600)
+    b.sync()
+    for i, (tx, _) in enumerate(singles):
+        assert np.array_equal(b.traces(i, "txx"), tx), i
+    b.close()
+
+
+def test_batch_rejects_a_bad_tile_shape():
+    from mixedprecisionfaracoustic_b200._abi import BiotError, BP_ERR_ARG
+    shots = config3_shots(seed=13, nshots=1, nt=20, precision="fp32", scale=0.05)
+    for bad in ((3, 1), (8, 8), (64, 1), (2, 1)):
+        with pytest.raises(BiotError) as e:
+            Batch([c for c, _ in shots], [m for _, m in shots], tile=bad)
+        assert e.value.code == BP_ERR_ARG

@@ -92,3 +92,127 @@ def test_create_refuses_a_time_step_above_the_stability_limit():
         s.run(cfg.nt)
         s.sync()
         assert np.isfinite(s.traces("txx")).all() and np.abs(s.traces("txx")).max() > 0
+
+
+# ---- injected allocation failures (host-side fake of an exhausted device) ----
+def _free_bytes():
+    import torch
+    torch.cuda.synchronize()
+    return torch.cuda.mem_get_info()[0]
+
+
+def leak_sized(prec="fp32"):
+    """A shot whose arena (~100 MB) dwarfs the driver's own small allocations."""
+    return config1(precision=prec, nx=1400, nz=700, nt=40, npml=10, nrec=30)
+
+
+LEAK_SLACK = 8 << 20     # bytes of device memory the driver may take for itself (streams, events)
+
+
+@pytest.mark.parametrize("nth", [1, 2])
+def test_create_out_of_memory_leaves_nothing_behind(nth):
+    """bp_create whose arena block (nth = 1) or medium staging block (nth = 2)
+    cannot be had returns BP_ERR_OOM and holds no device memory afterwards; the
+    next create on the same device works and gives the usual results."""
+    lib = _abi.load()
+    cfg, med = leak_sized()
+    with Simulation(cfg, med) as s:      # first: loads the kernels, fills the cache
+        s.run(cfg.nt)
+        want = s.traces("txx")
+    assert lib.bp_release_cached_memory(-1) == _abi.BP_OK
+    before = _free_bytes()
+    assert lib.bp_debug_fail_allocation(nth) == _abi.BP_OK
+    try:
+        with pytest.raises(BiotError) as e:
+            Simulation(cfg, med)
+        assert e.value.code == _abi.BP_ERR_OOM, str(e.value)
+    finally:
+        lib.bp_debug_fail_allocation(0)
+    assert lib.bp_release_cached_memory(-1) == _abi.BP_OK
+    assert abs(_free_bytes() - before) <= LEAK_SLACK
+    with Simulation(cfg, med) as s:
+        s.run(cfg.nt)
+        assert np.array_equal(s.traces("txx"), want)
+
+
+def test_batch_create_out_of_memory_releases_the_shots_already_made():
+    lib = _abi.load()
+    shots = [leak_sized() for _ in range(3)]
+    Batch([c for c, _ in shots[:1]], [m for _, m in shots[:1]]).close()     # warm: kernels, streams
+    assert lib.bp_release_cached_memory(-1) == _abi.BP_OK
+    before = _free_bytes()
+    assert lib.bp_debug_fail_allocation(5) == _abi.BP_OK   # the third shot's arena block
+    try:
+        with pytest.raises(BiotError) as e:
+            Batch([c for c, _ in shots], [m for _, m in shots])
+        assert e.value.code == _abi.BP_ERR_OOM, str(e.value)
+    finally:
+        lib.bp_debug_fail_allocation(0)
+    assert lib.bp_release_cached_memory(-1) == _abi.BP_OK
+    assert abs(_free_bytes() - before) <= LEAK_SLACK
+
+
+def test_server_request_fails_on_allocation_failure_and_the_rest_run():
+    """A request whose shot cannot get its device memory at admission ends as
+    failed and gives its budget back; the requests after it run normally and
+    give the results they give alone."""
+    lib = _abi.load()
+    cfg, med = healthy()
+    with Simulation(cfg, med) as s:
+        s.run(cfg.nt)
+        want = s.traces("txx")
+    srv = Server(hbm_budget_bytes=4 << 30, steps_per_sync=20)
+    try:
+        assert lib.bp_debug_fail_allocation(1) == _abi.BP_OK
+        bad = srv.submit(cfg, med)
+        srv.wait(bad, 120)
+        assert srv.poll(bad) == "failed"
+        lib.bp_debug_fail_allocation(0)
+        good = srv.submit(cfg, med)
+        srv.wait(good, 120)
+        assert srv.poll(good) == "done"
+        assert np.array_equal(srv.traces(good, "txx"), want)
+        st = srv.stats()
+        assert st["failed"] == 1 and st["completed"] == 1 and st["hbm_in_use"] == 0
+    finally:
+        lib.bp_debug_fail_allocation(0)
+        srv.close()
+
+
+def test_server_cancel_of_a_queued_and_of_a_resident_request():
+    """bp_server_cancel on a request that is still queued (the budget holds one
+    request at a time) and on one that is resident: both end as cancelled,
+    their budget comes back, and the request that was not cancelled finishes
+    with the result it gives alone."""
+    from mixedprecisionfaracoustic_b200.biot import shot_bytes
+    import time
+    long_cfg, long_med = config1(precision="fp32", nx=400, nz=200, nt=4000, npml=10, nrec=20)
+    cfg, med = healthy()
+    with Simulation(cfg, med) as s:
+        s.run(cfg.nt)
+        want = s.traces("txx")
+    budget = max(shot_bytes(long_cfg), shot_bytes(cfg)) + (1 << 20)
+    srv = Server(hbm_budget_bytes=budget, steps_per_sync=10)
+    try:
+        resident = srv.submit(long_cfg, long_med)
+        queued = srv.submit(long_cfg, long_med)
+        ok = srv.submit(cfg, med)
+        t0 = time.time()
+        while srv.poll(resident) != "running":
+            assert time.time() - t0 < 60
+            time.sleep(0.01)
+        assert srv.poll(queued) == "queued"
+        srv.cancel(queued)
+        srv.cancel(resident)
+        for rid in (resident, queued, ok):
+            srv.wait(rid, 300)
+        assert srv.poll(resident) == "cancelled" and srv.poll(queued) == "cancelled"
+        assert srv.poll(ok) == "done"
+        assert np.array_equal(srv.traces(ok, "txx"), want)
+        with pytest.raises(BiotError) as e:
+            srv.traces(resident, "txx")
+        assert e.value.code == _abi.BP_ERR_STATE
+        st = srv.stats()
+        assert st["cancelled"] == 2 and st["completed"] == 1 and st["hbm_in_use"] == 0
+    finally:
+        srv.close()

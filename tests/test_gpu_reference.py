@@ -100,3 +100,25 @@ def test_comp16_reference_run_vs_fp64():
             assert a.trace_rel_l2(b, c) <= 1e-3, c
         sc = a.scaling()
     assert sc["em"] == -23          # method.md worked example for this medium
+
+
+def test_dropin_binary_writes_the_reference_files(ref_run, golden, tmp_path):
+    """The shipped drop-in program (bin/biot_reference_run, the C++ driver over
+    the C ABI) run for 501 steps: its snapshot files match the reference's
+    golden slices, and every file it writes is byte-identical to the files
+    bp_write_reference_outputs wrote for the same run through Python."""
+    import subprocess
+    from conftest import ROOT
+    exe = ROOT / "mixedprecisionfaracoustic_b200" / "bin" / "biot_reference_run"
+    assert exe.exists(), exe
+    r = subprocess.run([str(exe), "--nt", "501", "--out", str(tmp_path)], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert "time loop" in r.stdout
+    _, py_out = ref_run
+    names = sorted(p.name for p in py_out.iterdir())
+    assert sorted(p.name for p in tmp_path.iterdir()) == names
+    for n in names:
+        assert (tmp_path / n).read_bytes() == (py_out / n).read_bytes(), n
+    for f in ("txx", "vux", "vuz", "vwx", "vwz"):
+        assert rel_l2(_parse(tmp_path / f"{f}500.dat"), golden[f + "500"]) <= 1e-5, f

@@ -68,3 +68,20 @@ def test_config3_and_4():
     nts = [c.nt for c, _ in reqs]
     assert 1000 <= min(nts) and max(nts) <= 6000
     assert {c.dim for c, _ in reqs} == {2, 3}
+
+
+def test_host_builder_is_bit_identical_to_the_library():
+    """The benchmark's CPU reference arm forms its medium without the CUDA
+    library; its values must be the library's bit for bit."""
+    from mixedprecisionfaracoustic_b200.presets import c0_coefficients
+    for seed in (1, 2, 3, 1000, 5000):
+        h, _ = layered_coefficients(seed, host=True)
+        lib, _ = layered_coefficients(seed, host=False)
+        assert h == lib, seed
+    assert c0_coefficients(host=True) == c0_coefficients(host=False)
+    a, _ = config1(nx=64, nz=48, nt=10, host=True)
+    b, mb = config1(nx=64, nz=48, nt=10)
+    _, ma = config1(nx=64, nz=48, nt=10, host=True)
+    assert a.pml_v0 == b.pml_v0
+    for k in ma:
+        assert np.array_equal(ma[k], mb[k]), k

@@ -69,3 +69,43 @@ def test_noalloc_on_seismograms():
     assert rc_a == 0 and rc_b == 0
     assert 0 < a < 1e-3
     assert abs(a - b) <= 1e-12 * a
+
+
+def test_noalloc_works_with_no_device_memory_left():
+    """The property the entry point exists for: it needs no device memory of
+    its own.  After a first call (which loads the kernels and looks up the
+    scratch array), the test takes every free byte of the device through torch,
+    as a process that hands all memory to its own pool does; the call must
+    still succeed and give the same value twice.  The allocating entry point
+    is then expected to fail for lack of memory (reported, not required: the
+    last partial page may still hold its small scratch)."""
+    import torch
+    lib = _abi.load()
+    n = 1 << 20
+    g = torch.Generator(device="cuda").manual_seed(7)
+    x = torch.randn(n, device="cuda", dtype=torch.float32, generator=g)
+    r = x + 1e-3 * torch.randn(n, device="cuda", dtype=torch.float32, generator=g)
+    rc, want = _call(lib.bp_rel_l2_device_noalloc, x, r)
+    assert rc == _abi.BP_OK
+    torch.cuda.synchronize()
+    hold = []
+    try:
+        for chunk in (1 << 30, 1 << 26, 1 << 22, 1 << 20):     # bytes; the last from 2 MB segments
+            while True:
+                try:
+                    hold.append(torch.empty(chunk, dtype=torch.uint8, device="cuda"))
+                except torch.OutOfMemoryError:
+                    break
+        free, _ = torch.cuda.mem_get_info()
+        assert free < (64 << 20), free
+        got = []
+        for _ in range(2):
+            rc, v = _call(lib.bp_rel_l2_device_noalloc, x, r)
+            assert rc == _abi.BP_OK, lib.bp_last_error()
+            got.append(v)
+        assert got[0] == want and got[1] == want, (got, want)
+        rc_alloc, _ = _call(lib.bp_rel_l2_device, x, r)
+        print(f"free bytes while full: {free}; allocating entry point rc = {rc_alloc}")
+    finally:
+        hold.clear()
+        torch.cuda.empty_cache()
