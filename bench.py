@@ -209,22 +209,33 @@ def run_ours(args, rank, ws):
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             ms = float(t.item())
         (bv, bt), cells = s.algorithmic_bytes()
-        pv, pt, pp = s.profile_phases(P)
-        dom = "v_phase" if pv >= pt else "t_phase"
-        t_dom = max(pv, pt)
-        b_dom = (bv if pv >= pt else bt) * cells
+        family = s.kernel()
+        if family == "fused":
+            # one launch per step: the fused kernel is the dominant (only) kernel
+            fms, fbpc = s.profile_fused(P)
+            pv, pt, pp = fms, 0.0, 0.0
+            dom, t_dom, b_dom = "fused_step", fms, fbpc * cells
+            bv, bt = fbpc, 0.0
+        else:
+            pv, pt, pp = s.profile_phases(P)
+            dom = "v_phase" if pv >= pt else "t_phase"
+            t_dom = max(pv, pt)
+            b_dom = (bv if pv >= pt else bt) * cells
         achieved = b_dom / (t_dom * 1e-3) / 1e9
         res[prec] = {
+            "kernel_family": family,
             "value": cells * K * ws / (ms * 1e-3) / 1e6,
             "ms_per_step": ms / K,
             "timed_regions": {"count": reps, "steps_each": K, "ms_min": min(regions), "ms_median": ms,
                               "ms_max": max(regions)},
             "launches": launches,
             "clocks": clk.summary(),
-            "phase_ms": {"v_phase": pv, "t_phase": pt, "record_inject": pp},
+            "phase_ms": ({"fused_step": pv} if family == "fused" else
+                         {"v_phase": pv, "t_phase": pt, "record_inject": pp}),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "bytes_per_cell": {"v_phase": bv, "t_phase": bt},
+                         "bytes_per_cell": ({"fused_step": bv} if family == "fused" else
+                                            {"v_phase": bv, "t_phase": bt}),
                          "step_frac": (bv + bt) * cells / ((pv + pt) * 1e-3) / 1e9 / peak},
             "cells": cells,
         }

@@ -178,7 +178,14 @@ int bp_set_graph_steps(bp_sim* sim, int steps);
 #define BP_KERNEL_REGISTER 1
 #define BP_KERNEL_STAGED 2
 #define BP_KERNEL_MARCH 3
+#define BP_KERNEL_FUSED 4   /* one launch per step (V, T, record, inject) from one copy
+                               of the state into a second one: 2D FP32/COMP16, fast
+                               rounding, receivers and source inside the stencil
+                               border; steps run in pairs, an odd last step of a
+                               bp_run by the register kernels */
 int bp_set_kernel(bp_sim* sim, int variant);
+/* The family that runs the steps (BP_KERNEL_REGISTER .. BP_KERNEL_FUSED). */
+int bp_get_kernel(bp_sim* sim, int* variant);
 
 /* Step index of the next step to run (it). */
 int bp_get_step(bp_sim* sim, int* it);
@@ -266,6 +273,13 @@ int bp_restore(bp_sim* sim, const void* host, size_t bytes);
  * ms[0] = V phase (velocity + its CPML), ms[1] = T phase (stress, pressure +
  * CPML), ms[2] = record + inject.  The steps are real steps (state advances). */
 int bp_profile_phases(bp_sim* sim, int nsteps, float ms[3]);
+
+/* The fused step kernel's mean device time per launch (ms) over nsteps real
+ * steps (rounded up to whole pairs), with CUDA events around each launch, and
+ * the algorithmic HBM bytes of one fused step per updated cell (every field
+ * read once and written once, every coefficient read once).  BP_ERR_ARG where
+ * the fused kernel does not apply (3D, FP64, reference rounding). */
+int bp_profile_fused(bp_sim* sim, int nsteps, float* ms, double* bytes_per_cell);
 
 /* Algorithmic HBM bytes per updated cell of each phase (the roofline
  * numerator) and the number of updated cells per step. */
@@ -357,7 +371,9 @@ typedef struct bp_tune {
     int tile_segs;        /* 128-cell x segments per tile, 1..4 (0 = 1)        */
     int tile_tz;          /* 3D: z planes among the tile's rows, 1..tile_rows
                              (0 = the precision's default)                    */
-    int reserved[3];
+    int kernel;           /* BP_KERNEL_* family; 0 = autotune (2D FP32/COMP16:
+                             the register tiles or the fused step kernel)     */
+    int reserved[2];
 } bp_tune;
 
 /* All shots must share dim, order and precision; sizes, media, sources and
@@ -374,9 +390,9 @@ int bp_batch_run_timed(bp_batch* b, int nsteps, float* ms);
 int bp_batch_get_traces(bp_batch* b, int shot, int comp, float* host, size_t n);
 int bp_batch_get_tune(bp_batch* b, bp_tune* chosen);
 /* Runs the autotuner now (it otherwise runs inside the first bp_batch_run):
- * times real steps of the batch, at most budget_steps of them, under candidate
- * tile shapes, then persistent CTAs per SM, then steps per sync, and keeps
- * the fastest; results are cached per (dim, order, precision, rounding, grid
+ * times real steps of the batch, at most budget_steps of them, under the
+ * candidate kernel families, then (register tiles) tile shapes and persistent
+ * CTAs per SM, then steps per sync, and keeps the fastest; results are cached per (dim, order, precision, rounding, grid
  * class) for the process.  The timed steps advance the shots.  No-op when the
  * bp_tune given to bp_batch_create fixed every setting.  (No counterpart in
  * the reference, which has one fixed (16, 8, 1) block, Float/main.cu:26-28.) */

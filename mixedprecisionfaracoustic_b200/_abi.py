@@ -22,7 +22,7 @@ TRACES = ["txx", "tzz", "vux", "vwx", "p"]          # sisx sisz sisvu sisvw sisp
 TRACE = {n: i for i, n in enumerate(TRACES)}
 SRC_TAU, SRC_P = 1, 2
 ROUND = {"fast": 0, "reference": 1}
-KERNELS = {"auto": 0, "register": 1, "staged": 2, "march": 3}
+KERNELS = {"auto": 0, "register": 1, "staged": 2, "march": 3, "fused": 4}
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 COEFS = ["rho_x", "rho_y", "rho_z", "rhof", "cc1_x", "cc1_y", "cc1_z", "cc2_x", "cc2_y", "cc2_z",
          "C", "M", "H", "H2u", "mu_xy", "mu_xz", "mu_yz"]
@@ -54,7 +54,7 @@ class BpMedium(C.Structure):
 
 class BpTune(C.Structure):
     _fields_ = [("tile_rows", C.c_int), ("steps_per_sync", C.c_int), ("ctas_per_sm", C.c_int),
-                ("tile_segs", C.c_int), ("tile_tz", C.c_int), ("reserved", C.c_int * 3)]
+                ("tile_segs", C.c_int), ("tile_tz", C.c_int), ("kernel", C.c_int), ("reserved", C.c_int * 2)]
 
 
 class BpServerStats(C.Structure):
@@ -74,6 +74,8 @@ _SIGS = [
     ("bp_run_timed", C.c_int, [C.c_void_p, C.c_int, FloatP]),
     ("bp_set_graph_steps", C.c_int, [C.c_void_p, C.c_int]),
     ("bp_set_kernel", C.c_int, [C.c_void_p, C.c_int]),
+    ("bp_get_kernel", C.c_int, [C.c_void_p, IntP]),
+    ("bp_profile_fused", C.c_int, [C.c_void_p, C.c_int, FloatP, DoubleP]),
     ("bp_get_step", C.c_int, [C.c_void_p, IntP]),
     ("bp_get_traces", C.c_int, [C.c_void_p, C.c_int, FloatP, C.c_size_t]),
     ("bp_get_snapshot", C.c_int, [C.c_void_p, C.c_int, C.c_int, FloatP, C.c_size_t]),

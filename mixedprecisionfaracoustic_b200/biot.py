@@ -192,8 +192,21 @@ class Simulation:
         return ms.value
 
     def set_kernel(self, variant: str) -> None:
-        """Phase-kernel family: 'auto', 'register' or 'staged' (TMA, 2D FP32/COMP16)."""
+        """Kernel family: 'auto', 'register', 'staged', 'march' or 'fused' (the
+        last three 2D FP32/COMP16 only)."""
         check(self.lib.bp_set_kernel(self.h, _abi.KERNELS[variant]), "bp_set_kernel")
+
+    def kernel(self) -> str:
+        """The kernel family that runs the steps."""
+        v = C.c_int()
+        check(self.lib.bp_get_kernel(self.h, C.byref(v)), "bp_get_kernel")
+        return {k: n for n, k in _abi.KERNELS.items()}[v.value]
+
+    def profile_fused(self, nsteps: int) -> tuple:
+        """(ms per fused-kernel launch, algorithmic bytes per cell of one fused step)."""
+        ms, b = C.c_float(), C.c_double()
+        check(self.lib.bp_profile_fused(self.h, int(nsteps), C.byref(ms), C.byref(b)), "bp_profile_fused")
+        return ms.value, b.value
 
     def set_graph_steps(self, steps: int) -> None:
         """Steps per captured CUDA graph (0: direct launches)."""
@@ -329,9 +342,10 @@ class Batch:
     """Many shots advanced by the same launches (bp_batch)."""
 
     def __init__(self, cfgs: Sequence[ShotConfig], media: Sequence[Medium], steps_per_sync: int = 0,
-                 ctas_per_sm: int = 0, tile: Optional[tuple] = None):
-        """tile = (rows, segs[, tz]) fixes the register kernels' tile shape;
-        None leaves it (and any other 0 setting) to the autotuner."""
+                 ctas_per_sm: int = 0, tile: Optional[tuple] = None, kernel: str = "auto"):
+        """tile = (rows, segs[, tz]) fixes the register kernels' tile shape and
+        kernel the family ('register', 'fused'); None / 'auto' (and any other 0
+        setting) leave it to the autotuner."""
         self.lib = load()
         self.cfgs = list(cfgs)
         carr = (BpConfig * len(cfgs))(*[c.to_c() for c in cfgs])
@@ -341,6 +355,7 @@ class Batch:
         if tile is not None:
             t.tile_rows, t.tile_segs = tile[0], tile[1]
             t.tile_tz = tile[2] if len(tile) > 2 else 0
+        t.kernel = _abi.KERNELS[kernel]
         h = C.c_void_p()
         check(self.lib.bp_batch_create(carr, marr, len(cfgs), C.byref(t), C.byref(h)), "bp_batch_create")
         self.h = h
@@ -368,7 +383,8 @@ class Batch:
         t = BpTune()
         check(self.lib.bp_batch_get_tune(self.h, C.byref(t)), "bp_batch_get_tune")
         return {"tile_rows": t.tile_rows, "tile_segs": t.tile_segs, "tile_tz": t.tile_tz,
-                "steps_per_sync": t.steps_per_sync, "ctas_per_sm": t.ctas_per_sm}
+                "steps_per_sync": t.steps_per_sync, "ctas_per_sm": t.ctas_per_sm,
+                "kernel": {k: n for n, k in _abi.KERNELS.items()}[t.kernel]}
 
     def autotune(self, budget_steps: int) -> dict:
         """Runs the autotuner now within budget_steps (real) steps; returns the choice."""

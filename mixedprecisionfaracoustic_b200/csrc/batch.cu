@@ -47,7 +47,8 @@ int BatchCore::rebuild() {
     std::vector<ShotDesc> h(n);
     long long t0 = 0;
     int maxrec = 0;
-    long long t0s = 0, t0m = 0;
+    long long t0s = 0, t0m = 0, t0f = 0;
+    bool all_fused = true;
     const TileShape ts = effective_shape();
     for (int i = 0; i < n; i++) {
         h[i] = shots[i]->desc;
@@ -55,7 +56,10 @@ int BatchCore::rebuild() {
         h[i].tile0 = t0;
         h[i].tile0s = t0s;
         h[i].tile0m = t0m;
+        h[i].tile0f = t0f;
         h[i].done = 0;
+        t0f += shots[i]->ntiles_f;
+        all_fused = all_fused && shots[i]->ntiles_f > 0;
         t0 += tiles;
         t0s += shots[i]->ntiles_s;
         t0m += shots[i]->ntiles_m;
@@ -69,6 +73,8 @@ int BatchCore::rebuild() {
     run.post_in_t = true;
     for (auto& sh : shots) run.post_in_t = run.post_in_t && sh->post_in_t;
     run.rounding = rounding;
+    run.ntiles_f = all_fused ? t0f : 0;
+    run.variant = kernel;
     run.multi_unit = ts.rows * ts.segs > phase_threads() / 32;
     run.configure(prec, dim, order, d_descs, n, t0, t0s, t0m, maxrec, st, ctas_per_sm,
                   steps_per_sync > 0 ? steps_per_sync : 32);
@@ -119,6 +125,7 @@ int BatchCore::autotune(int budget_steps) {
     TuneKey key{dim, order, prec + 16 * rounding, (int)std::floor(std::log2((double)std::max(cells, 1LL))),
                 (int)std::floor(std::log2((double)shots.size()))};
     const bool fix_shape = shape.rows > 0, fix_c = ctas_per_sm > 0, fix_s = steps_per_sync > 0;
+    const bool fix_k = kernel != BP_KERNEL_AUTO;
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         auto it = tune_cache().find(key);
@@ -126,6 +133,7 @@ int BatchCore::autotune(int budget_steps) {
             if (!fix_c) ctas_per_sm = it->second.ctas_per_sm;
             if (!fix_s) steps_per_sync = it->second.steps_per_sync;
             if (!fix_shape) shape = it->second.shape;
+            if (!fix_k) kernel = it->second.kernel;
             tuned = true;
             return rebuild();
         }
@@ -138,14 +146,15 @@ int BatchCore::autotune(int budget_steps) {
     cudaEventCreate(&b);
     int used = 0;
     double best = 1e30;
-    TuneVal bv{ctas_per_sm, fix_s ? steps_per_sync : 32, effective_shape()};
+    TuneVal bv{ctas_per_sm, fix_s ? steps_per_sync : 32, effective_shape(), fix_k ? kernel : BP_KERNEL_REGISTER};
     // times one candidate; false if it no longer fits the step budget
-    auto trial = [&](int c, int sps, TileShape ts, int* rc) -> bool {
+    auto trial = [&](int c, int sps, TileShape ts, int kern, int* rc) -> bool {
         const int steps = std::max(sps, 16);
         if (used + sps + steps > budget) return false;
         ctas_per_sm = c;
         steps_per_sync = sps;
         shape = ts;
+        kernel = kern;
         *rc = rebuild();
         if (*rc) return false;
         advance(sps);                          // warm: captures the graph
@@ -158,16 +167,26 @@ int BatchCore::autotune(int budget_steps) {
         float ms = 0;
         cudaEventElapsedTime(&ms, a, b);
         const double per = ms / steps;
-        if (per < best) { best = per; bv = TuneVal{c, sps, ts}; }
+        if (per < best) { best = per; bv = TuneVal{c, sps, ts, kern}; }
         return true;
     };
     int rc = BP_OK;
-    // stage 1: tile shape (at the current CTA count and 32 steps per sync)
-    if (!fix_shape)
+    // stage 0: kernel family (2D FP32/COMP16: the fused step kernel against the
+    // register tiles at their default shape)
+    bool can_fused = fused_supported(prec, dim) && rounding == BP_ROUND_FAST;
+    for (auto& s : shots) can_fused = can_fused && s->ntiles_f > 0;
+    if (!fix_k && can_fused) {
+        const TuneVal base = bv;
+        for (int kern : {BP_KERNEL_REGISTER, BP_KERNEL_FUSED})
+            if (!trial(base.ctas_per_sm, base.steps_per_sync, base.shape, kern, &rc) && rc) break;
+    }
+    // stage 1: tile shape of the register kernels (at the current CTA count and 32 steps per sync)
+    if (!rc && !fix_shape && bv.kernel != BP_KERNEL_FUSED)
         for (const TileShape& ts : shape_candidates(dim, prec))
-            if (!trial(bv.ctas_per_sm, bv.steps_per_sync, ts, &rc) && rc) break;
-    // stage 2: persistent CTAs per SM
-    if (!rc && !fix_c) {
+            if (!(best < 1e30 && ts.rows == bv.shape.rows && ts.segs == bv.shape.segs && ts.tz == bv.shape.tz))
+                if (!trial(bv.ctas_per_sm, bv.steps_per_sync, ts, bv.kernel, &rc) && rc) break;
+    // stage 2: persistent CTAs per SM (register tiles)
+    if (!rc && !fix_c && bv.kernel != BP_KERNEL_FUSED) {
         const int occ = std::min(phase_occupancy(prec, dim, order, true, rounding),
                                  phase_occupancy(prec, dim, order, false, rounding));
         std::vector<int> ctas = {0};
@@ -175,15 +194,15 @@ int BatchCore::autotune(int budget_steps) {
         if (occ >= 3) ctas.push_back(1);
         const TuneVal base = bv;
         for (int c : ctas)
-            if (!(c == base.ctas_per_sm && !fix_shape && best < 1e30))
-                if (!trial(c, base.steps_per_sync, base.shape, &rc) && rc) break;
+            if (!(c == base.ctas_per_sm && best < 1e30))
+                if (!trial(c, base.steps_per_sync, base.shape, base.kernel, &rc) && rc) break;
     }
     // stage 3: steps per graph replay
     if (!rc && !fix_s) {
         const TuneVal base = bv;
         for (int sps : {8, 32, 128})
             if (sps != base.steps_per_sync || best >= 1e30)
-                if (!trial(base.ctas_per_sm, sps, base.shape, &rc) && rc) break;
+                if (!trial(base.ctas_per_sm, sps, base.shape, base.kernel, &rc) && rc) break;
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -191,6 +210,7 @@ int BatchCore::autotune(int budget_steps) {
     ctas_per_sm = bv.ctas_per_sm;
     steps_per_sync = bv.steps_per_sync;
     shape = bv.shape;
+    kernel = bv.kernel;
     tuned = true;
     if (best < 1e30) {
         std::lock_guard<std::mutex> g(g_tune_mu);
@@ -260,9 +280,19 @@ int bp_batch_create(const bp_config* cfgs, const bp_medium* media, int nshots, c
             }
             b->core.shape = t;
         }
+        if (tune->kernel < BP_KERNEL_AUTO || tune->kernel > BP_KERNEL_FUSED ||
+            (tune->kernel == BP_KERNEL_FUSED && !(fused_supported(cfgs[0].precision, cfgs[0].dim) &&
+                                                 cfgs[0].rounding == BP_ROUND_FAST))) {
+            set_error("bad kernel family for this batch");
+            cudaStreamDestroy(b->st);
+            delete b;
+            return BP_ERR_ARG;
+        }
+        b->core.kernel = tune->kernel;
         b->core.ctas_per_sm = tune->ctas_per_sm;
         b->core.steps_per_sync = tune->steps_per_sync;
-        b->user_tuned = tune->ctas_per_sm > 0 && tune->steps_per_sync > 0 && tune->tile_rows > 0;
+        b->user_tuned = tune->ctas_per_sm > 0 && tune->steps_per_sync > 0 && tune->tile_rows > 0 &&
+                        tune->kernel != BP_KERNEL_AUTO;
     }
     for (int i = 0; i < nshots; i++) {
         auto sh = std::make_unique<Shot>();
@@ -363,6 +393,7 @@ int bp_batch_get_tune(bp_batch* b, bp_tune* chosen) {
     chosen->tile_tz = b->core.dim == 3 ? t.tz : 1;
     chosen->steps_per_sync = b->core.steps_per_sync;
     chosen->ctas_per_sm = b->core.ctas_per_sm;
+    chosen->kernel = b->core.run.family();
     return BP_OK;
 }
 

@@ -20,6 +20,7 @@ struct TuneKey {
 struct TuneVal {
     int ctas_per_sm, steps_per_sync;
     TileShape shape;
+    int kernel;
 };
 
 // Process-wide cache of autotuning results keyed by (dim, order, precision
@@ -38,6 +39,7 @@ struct BatchCore {
     Runner run;
     int ctas_per_sm = 0, steps_per_sync = 0;    // 0 = autotune
     TileShape shape{0, 0, 0};                   // rows 0 = autotune (default shape until tuned)
+    int kernel = BP_KERNEL_AUTO;                // family; AUTO = autotune (library default until tuned)
     bool tuned = false;
     long long cell_updates = 0;
 

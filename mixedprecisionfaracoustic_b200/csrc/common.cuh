@@ -109,6 +109,15 @@ struct ShotDesc {
     // rec_row[key + 1]), sorted by x, each as (x, unique receiver index)
     const int* rec_row;
     const int2* rec_xu;
+    // second copy of the state for the fused step kernel (2D FP32/COMP16): the
+    // fields (and residuals) and the V-phase memory variables; steps alternate
+    // between the two copies in pairs, so the first copy is current between
+    // pairs.  Tasks: columns of 120 cells x segments of zseg_f rows.
+    void* fb[BP_NFIELDS];
+    int8_t* flob[BP_NFIELDS];
+    void* psiVb[3];
+    long long tile0f;             // first task of this shot in the fused tiling
+    int ncol_f, zseg_f, nzs_f, pad_f;
     template <class R>
     __device__ __forceinline__ R dtr() const { return sizeof(R) == 8 ? (R)dtd : (R)dt; }
 };
@@ -188,6 +197,10 @@ struct PolF32 {
     __device__ __forceinline__ static void st1(void* p, int8_t*, cidx i, real v) {
         static_cast<float*>(p)[i] = v;
     }
+    // store (if st) and leave in v the value a later load returns
+    __device__ __forceinline__ static void st4_rt(void* p, int8_t* lo, cidx i, real (&v)[4], bool st) {
+        if (st) st4(p, lo, i, v);
+    }
     // raw (undecoded) loads, for kernels that issue loads well before use
     using raw4 = float4;
     using raw1 = float;
@@ -226,6 +239,9 @@ struct PolF64 {
     }
     __device__ __forceinline__ static void st1(void* p, int8_t*, cidx i, real v) {
         static_cast<double*>(p)[i] = v;
+    }
+    __device__ __forceinline__ static void st4_rt(void* p, int8_t* lo, cidx i, real (&v)[4], bool st) {
+        if (st) st4(p, lo, i, v);
     }
     struct raw4 { double2 a, b; };
     using raw1 = double;
@@ -300,6 +316,23 @@ struct PolC16 {
         encode_ch(v, h, l);
         static_cast<__half*>(p)[i] = h;
         lo[i] = l;
+    }
+    // store (if st) and leave in v the decoded stored value, as a later load returns it
+    __device__ __forceinline__ static void st4_rt(void* p, int8_t* lo, cidx i, real (&v)[4], bool st) {
+        __half hs[4];
+        int8_t ls[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) encode_ch(v[j], hs[j], ls[j]);
+        if (st) {
+            uint2 h;
+            __half2 a = __halves2half2(hs[0], hs[1]), b = __halves2half2(hs[2], hs[3]);
+            h.x = *reinterpret_cast<unsigned*>(&a);
+            h.y = *reinterpret_cast<unsigned*>(&b);
+            *reinterpret_cast<uint2*>(static_cast<__half*>(p) + i) = h;
+            *reinterpret_cast<char4*>(lo + i) = make_char4(ls[0], ls[1], ls[2], ls[3]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) v[j] = decode_ch(hs[j], ls[j]);
     }
     // raw loads: the fp16 words and the residual bytes (zero residuals where
     // the array has none, which decodes to the same value as hi alone)

@@ -1,8 +1,11 @@
 // runner.h - issues chunks of time steps for a set of shot descriptors, either
 // as direct launches or by replaying a captured CUDA graph of S steps.
 //
-// 2D FP32/COMP16 phases run the TMA-staged kernels (step_staged.cu, one
-// persistent CTA per SM); 3D and FP64 phases the register kernels (step.cu).
+// Kernel families: the register tile kernels (step.cu: a V-phase and a
+// T-phase launch per step, every dim and precision), and for 2D FP32/COMP16
+// the fused step kernel (step_fused.cu: one launch per step, steps in pairs,
+// an odd last step of a chunk by the tile kernels), the marching kernels
+// (step_march.cu) and the bulk-copy staged kernels (step_staged.cu).
 #pragma once
 #include "shot.h"
 
@@ -29,6 +32,10 @@ struct Runner {
     bool post_in_t = false;            // every shot's receivers and source lie in cells the T phase visits
     int rounding = BP_ROUND_FAST;      // FP32 BP_ROUND_REFERENCE: PolF32R register kernels only
     bool multi_unit = false;           // the shots' tile shape has more units than a CTA has warps
+    long long ntiles_f = 0;            // tasks of the fused step kernel (0: some shot cannot take it)
+    int grid_f = 1;
+    bool fused = false;
+    long long graph_launches = 0;      // kernels one replay of the captured graph runs
 
     void configure(int prec_, int dim_, int order_, const ShotDesc* d, int n, long long tiles, long long tiles_s,
                    long long tiles_m, int maxrec, cudaStream_t s, int ctas_per_sm, int steps_per_graph) {
@@ -44,6 +51,7 @@ struct Runner {
         grid_t = (int)(gt < tiles ? gt : (tiles > 0 ? tiles : 1));
         select_kernels();
         grid_s = (int)(sms < tiles_s ? sms : (tiles_s > 0 ? tiles_s : 1));
+        if (fused_supported(prec, dim)) grid_f = fused_occupancy(prec, order) * sms;
         if (!d_err) {
             // from the arena cache: a cudaFree, even of 4 bytes, stalled the
             // host for up to 0.6 s when the simulation was destroyed
@@ -54,10 +62,16 @@ struct Runner {
         reset_graph();
     }
     void select_kernels() {
+        const bool can_f = fused_supported(prec, dim) && ntiles_f > 0 && rounding == BP_ROUND_FAST;
+        fused = can_f && (variant == BP_KERNEL_FUSED || (variant == BP_KERNEL_AUTO && fused_default()));
         const bool can_m = march_supported(prec, dim) && ntiles_m > 0 && rounding == BP_ROUND_FAST;
-        march = can_m && (variant == BP_KERNEL_MARCH || (variant == BP_KERNEL_AUTO && march_default()));
+        march = !fused && can_m && (variant == BP_KERNEL_MARCH || (variant == BP_KERNEL_AUTO && march_default()));
         const bool can = staged_supported(prec, dim) && ntiles_s > 0 && rounding == BP_ROUND_FAST;
-        staged = !march && can && (variant == BP_KERNEL_STAGED || (variant == BP_KERNEL_AUTO && staged_default()));
+        staged = !fused && !march && can &&
+                 (variant == BP_KERNEL_STAGED || (variant == BP_KERNEL_AUTO && staged_default()));
+    }
+    int family() const {
+        return fused ? BP_KERNEL_FUSED : march ? BP_KERNEL_MARCH : staged ? BP_KERNEL_STAGED : BP_KERNEL_REGISTER;
     }
     void reset_graph() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -80,6 +94,7 @@ struct Runner {
 #endif
         return post_in_t && !march && !staged;
     }
+    // launches of one step of the two-phase kernels
     int launches_per_step() const { return fused_post() ? 2 : 3; }
     cudaError_t phase(bool v, int k) {
         if (march) return launch_phase_march(prec, order, v, d_shots, nshots, ntiles_m, k, st);
@@ -88,23 +103,46 @@ struct Runner {
                             (!v && fused_post()) ? 1 : 0, rounding, multi_unit);
     }
 
+    // One step (index k of the chunk) of the two-phase kernels.
+    cudaError_t tile_step(int k, long long* n) {
+        cudaError_t e = phase(true, k);
+        if (e == cudaSuccess) e = phase(false, k);
+        if (e == cudaSuccess && !fused_post()) e = launch_post(prec, d_shots, nshots, max_rec, k, 1, st);
+        *n += launches_per_step();
+        return e;
+    }
     // m steps issued directly (k = 0..m-1), then the step bases advance by m.
-    cudaError_t issue(int m, bool count = true) {
+    // The fused kernel takes the steps in pairs (copy A -> B -> A); an odd last
+    // step runs the two-phase kernels on copy A.  *n receives the launches.
+    cudaError_t issue(int m, long long* n) {
         cudaError_t e = cudaSuccess;
-        for (int k = 0; k < m && e == cudaSuccess; k++) {
-            e = phase(true, k);
-            if (e == cudaSuccess) e = phase(false, k);
-            if (e == cudaSuccess && !fused_post()) e = launch_post(prec, d_shots, nshots, max_rec, k, 1, st);
+        *n = 0;
+        for (int k = 0; k < m && e == cudaSuccess;) {
+            if (fused && k + 1 < m) {
+                e = launch_fused(prec, order, d_shots, nshots, ntiles_f, k, 0, grid_f, st);
+                if (e == cudaSuccess) e = launch_fused(prec, order, d_shots, nshots, ntiles_f, k + 1, 1, grid_f, st);
+                *n += 2;
+                k += 2;
+            } else {
+                e = tile_step(k, n);
+                k += 1;
+            }
         }
         if (e == cudaSuccess) e = launch_advance(d_shots, nshots, m, st);
-        if (count) launches += (long long)launches_per_step() * m + 1;
+        *n += 1;
+        return e;
+    }
+    cudaError_t issue(int m) {
+        long long n = 0;
+        cudaError_t e = issue(m, &n);
+        launches += n;
         return e;
     }
     cudaError_t ensure_graph() {
         if (exec || graph_failed || graph_steps <= 0) return cudaSuccess;
         cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) { graph_failed = true; cudaGetLastError(); return cudaSuccess; }
-        cudaError_t ei = issue(graph_steps, false);
+        cudaError_t ei = issue(graph_steps, &graph_launches);
         e = cudaStreamEndCapture(st, &graph);
         if (ei != cudaSuccess || e != cudaSuccess) { graph_failed = true; cudaGetLastError(); graph = nullptr; return cudaSuccess; }
         e = cudaGraphInstantiate(&exec, graph, 0);
@@ -118,7 +156,7 @@ struct Runner {
             ensure_graph();
             while (exec && m >= graph_steps && e == cudaSuccess) {
                 e = cudaGraphLaunch(exec, st);
-                launches += (long long)launches_per_step() * graph_steps + 1;
+                launches += graph_launches;
                 m -= graph_steps;
             }
         }

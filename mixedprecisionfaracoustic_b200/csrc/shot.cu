@@ -107,6 +107,8 @@ struct Plan {
     // offsets
     size_t o_f[BP_NFIELDS], o_flo[BP_NFIELDS], o_vc[VC_COUNT], o_vclo[VC_COUNT], o_tc[TC_COUNT], o_tclo[TC_COUNT];
     size_t o_prof[3][4], o_psiV[3], o_psiT[3];
+    size_t o_fb[BP_NFIELDS], o_flob[BP_NFIELDS], o_psiVb[3];   // second copy (fused step kernel)
+    bool fused;
     size_t o_tr, o_tr64, o_wav, o_dyn, o_rtab, o_rec, o_recrow, o_recxu, o_step, o_blowup, o_snap, o_scratch, o_out, o_desc;
     size_t total;
     size_t staging;               // transient medium upload
@@ -164,11 +166,16 @@ void make_plan(const bp_config* c, int nurec, Plan& p) {
             if ((m >> f & 1u) && field_used(dim, f)) p.ncapt++;
     }
     Arena A;
+    p.fused = fused_supported(prec, dim) && c->rounding == BP_ROUND_FAST;
     for (int f = 0; f < BP_NFIELDS; f++) {
-        p.o_f[f] = p.o_flo[f] = (size_t)-1;
+        p.o_f[f] = p.o_flo[f] = p.o_fb[f] = p.o_flob[f] = (size_t)-1;
         if (!field_used(dim, f)) continue;
         p.o_f[f] = A.take(p.ncell * p.fe);
         if (p.lo_f) p.o_flo[f] = A.take(p.ncell);
+        if (p.fused) {
+            p.o_fb[f] = A.take(p.ncell * p.fe);
+            if (p.lo_f) p.o_flob[f] = A.take(p.ncell);
+        }
     }
     for (int k = 0; k < VC_COUNT; k++) {
         p.o_vc[k] = p.o_vclo[k] = (size_t)-1;
@@ -184,10 +191,11 @@ void make_plan(const bp_config* c, int nurec, Plan& p) {
     }
     for (int a = 0; a < 3; a++) {
         for (int q = 0; q < 4; q++) p.o_prof[a][q] = (size_t)-1;
-        p.o_psiV[a] = p.o_psiT[a] = (size_t)-1;
+        p.o_psiV[a] = p.o_psiT[a] = p.o_psiVb[a] = (size_t)-1;
         if (a == 1 && dim == 2) continue;
         for (int q = 0; q < 4; q++) p.o_prof[a][q] = A.take((size_t)ns_ax[a] * p.re);
         p.o_psiV[a] = A.take((size_t)2 * p.ns * p.slab_cells[a] * p.re);
+        if (p.fused) p.o_psiVb[a] = A.take((size_t)2 * p.ns * p.slab_cells[a] * p.re);
         p.o_psiT[a] = A.take((size_t)2 * p.ns * p.slab_cells[a] * p.re);
     }
     const size_t tr = (size_t)BP_NTRACE * nurec * c->nt;
@@ -288,15 +296,24 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     S.nseg_s = (p.nx + staged_tile_width() - 1) / staged_tile_width();
     S.tile0m = 0;
     S.ncol_m = (p.nx + march_cells() - 1) / march_cells();
+    S.tile0f = 0;
+    S.ncol_f = fused_cols(p.nx);
     {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         S.zseg_m = march_zseg(S.ncol_m, p.nz - 2 * S.hw, sms);
+        S.zseg_f = fused_zseg(S.ncol_f, p.nz - 2 * S.hw, sms);
+        S.nzs_f = (p.nz - 2 * S.hw + S.zseg_f - 1) / S.zseg_f;
     }
     S.nt = c->nt;
     S.dt = c->dt; S.dtd = c->dt; S.h = c->dx; S.hd = c->dx; S.inv_h = 1.0f / c->dx;
-    for (int f = 0; f < BP_NFIELDS; f++) { S.f[f] = at(p.o_f[f]); S.flo[f] = (int8_t*)at(p.o_flo[f]); }
+    for (int f = 0; f < BP_NFIELDS; f++) {
+        S.f[f] = at(p.o_f[f]);
+        S.flo[f] = (int8_t*)at(p.o_flo[f]);
+        S.fb[f] = at(p.o_fb[f]);
+        S.flob[f] = (int8_t*)at(p.o_flob[f]);
+    }
     for (int k = 0; k < VC_COUNT; k++) { S.vc[k] = at(p.o_vc[k]); S.vclo[k] = (int8_t*)at(p.o_vclo[k]); }
     for (int k = 0; k < TC_COUNT; k++) { S.tc[k] = at(p.o_tc[k]); S.tclo[k] = (int8_t*)at(p.o_tclo[k]); }
     for (int a = 0; a < 3; a++) {
@@ -305,6 +322,7 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
         S.slab[a] = p.slab[a];
         S.slab_cells[a] = p.slab_cells[a];
         S.psiV[a] = at(p.o_psiV[a]);
+        S.psiVb[a] = at(p.o_psiVb[a]);
         S.psiT[a] = at(p.o_psiT[a]);
     }
     S.traces = (float*)at(p.o_tr);
@@ -454,6 +472,9 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     // while k_post spreads it over its own grid: measured on B200, 2000
     // receivers (4040 x 2040) are 1.2 % faster per step recorded in the T phase,
     // 65,536 (a 256 x 256 surface array on 552 x 552 x 424) 2.7 % slower
+    // the fused step kernel records and injects in its stress phase only, so it
+    // needs every receiver and the source in cells that phase visits
+    const bool rec_in_t = post_in_t;
     post_in_t = post_in_t && nurec <= 8192;
     if (e == cudaSuccess)
         e = cudaMemcpyAsync((void*)S.rec_row, row_start.data(), row_start.size() * 4, cudaMemcpyHostToDevice, st);
@@ -473,6 +494,7 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     cells = cx * cy * cz;
     ntiles_s = (long long)S.nseg_s * ((S.nrows + staged_tile_rows() - 1) / staged_tile_rows());
     ntiles_m = dim == 2 ? (long long)S.ncol_m * ((p.nz - 2 * S.hw + S.zseg_m - 1) / S.zseg_m) : 0;
+    ntiles_f = p.fused && rec_in_t ? (long long)S.ncol_f * S.nzs_f : 0;
     it_host = 0;
     return BP_OK;
 }

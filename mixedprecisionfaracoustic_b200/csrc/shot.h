@@ -55,6 +55,14 @@ int march_cells();
 int march_zseg(long long ncol, int nrows, int sms);
 cudaError_t launch_phase_march(int prec, int order, bool vphase, const ShotDesc* d, int nshots, long long ntasks,
                                int k, cudaStream_t st);
+// fused 2D step kernel (step_fused.cu): one launch per step, state copy par -> 1 - par
+bool fused_supported(int prec, int dim);
+bool fused_default();            // whether BP_KERNEL_AUTO picks the fused kernel where supported
+int fused_cols(int nx);
+int fused_zseg(long long ncol, int nrows, int sms);
+int fused_occupancy(int prec, int order);
+cudaError_t launch_fused(int prec, int order, const ShotDesc* d, int nshots, long long ntasks, int k, int par,
+                         int grid, cudaStream_t st);
 
 void host_pml_region(int n, int np, float H, int i, bool* left, bool* right);
 cudaError_t launch_profile(int prec, int n, int np, float H, double dt, double v0, double rc, void* b, void* e,
@@ -101,6 +109,7 @@ struct Shot {
     long long ntiles = 0;              // tiles of the register kernels (current TileShape)
     long long ntiles_s = 0;            // tiles of the TMA-staged 2D kernels (256 x staged_tile_rows)
     long long ntiles_m = 0;            // tasks of the marching 2D kernels (128 cells x zseg_m rows)
+    long long ntiles_f = 0;            // tasks of the fused 2D step kernel (120 cells x zseg_f rows), 0 = none
     bool post_in_t = false;            // receivers and source all in cells the T phase visits
 
     // The device regions that make up the shot's evolving state, in a fixed

@@ -144,6 +144,7 @@ int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out) {
     if (rc) { s->shot.destroy(); cudaStreamDestroy(s->st); delete s; return rc; }
     s->run.post_in_t = s->shot.post_in_t;
     s->run.rounding = cfg->rounding;
+    s->run.ntiles_f = s->shot.ntiles_f;
     s->run.configure(cfg->precision, cfg->dim, cfg->order, s->shot.d_desc, 1, s->shot.ntiles, s->shot.ntiles_s,
                      s->shot.ntiles_m, s->shot.nurec, s->st, 0, 32);
     *out = s;
@@ -220,7 +221,12 @@ int bp_set_graph_steps(bp_sim* s, int steps) {
 }
 
 int bp_set_kernel(bp_sim* s, int variant) {
-    if (!s || variant < BP_KERNEL_AUTO || variant > BP_KERNEL_MARCH) { set_error("bad arguments"); return BP_ERR_ARG; }
+    if (!s || variant < BP_KERNEL_AUTO || variant > BP_KERNEL_FUSED) { set_error("bad arguments"); return BP_ERR_ARG; }
+    if (variant == BP_KERNEL_FUSED && (s->shot.ntiles_f <= 0 || s->shot.cfg.rounding != BP_ROUND_FAST)) {
+        set_error("the fused step kernel covers 2D FP32 and COMP16 with fast rounding, receivers and source "
+                  "inside the stencil border");
+        return BP_ERR_ARG;
+    }
     if (variant == BP_KERNEL_STAGED && !staged_supported(s->shot.cfg.precision, s->shot.cfg.dim)) {
         set_error("the staged kernels cover 2D FP32 and COMP16 only");
         return BP_ERR_ARG;
@@ -507,7 +513,58 @@ int bp_algorithmic_bytes(bp_sim* s, double bpc[2], long long* cells) {
 
 int bp_launches_per_step(bp_sim* s, int* n) {
     if (!s || !n) { set_error("bad arguments"); return BP_ERR_ARG; }
-    *n = s->run.launches_per_step();
+    *n = s->run.fused ? 1 : s->run.launches_per_step();
+    return BP_OK;
+}
+
+int bp_get_kernel(bp_sim* s, int* variant) {
+    if (!s || !variant) { set_error("bad arguments"); return BP_ERR_ARG; }
+    *variant = s->run.family();
+    return BP_OK;
+}
+
+int bp_profile_fused(bp_sim* s, int nsteps, float* ms, double* bytes_per_cell) {
+    if (!s || !ms || nsteps < 1) { set_error("bad arguments"); return BP_ERR_ARG; }
+    Shot& sh = s->shot;
+    Runner& R = s->run;
+    if (sh.ntiles_f <= 0 || sh.cfg.rounding != BP_ROUND_FAST) {
+        set_error("the fused step kernel does not apply to this simulation");
+        return BP_ERR_ARG;
+    }
+    SIM_CK(cudaSetDevice(s->device));
+    const int pairs = std::min((nsteps + 1) / 2, (sh.cfg.nt - sh.it_host) / 2);
+    if (pairs < 1) { set_error("no steps left to profile"); return BP_ERR_STATE; }
+    cudaEvent_t ev[3];
+    for (auto& x : ev) SIM_CK(cudaEventCreate(&x));
+    double acc = 0;
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < pairs && e == cudaSuccess; i++) {
+        cudaEventRecord(ev[0], s->st);
+        e = launch_fused(R.prec, R.order, R.d_shots, R.nshots, R.ntiles_f, 0, 0, R.grid_f, s->st);
+        cudaEventRecord(ev[1], s->st);
+        if (e == cudaSuccess) e = launch_fused(R.prec, R.order, R.d_shots, R.nshots, R.ntiles_f, 1, 1, R.grid_f, s->st);
+        cudaEventRecord(ev[2], s->st);
+        if (e == cudaSuccess) e = launch_advance(R.d_shots, R.nshots, 2, s->st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[2]);
+        float t0 = 0, t1 = 0;
+        if (e == cudaSuccess) {
+            cudaEventElapsedTime(&t0, ev[0], ev[1]);
+            cudaEventElapsedTime(&t1, ev[1], ev[2]);
+            acc += t0 + t1;
+        }
+        R.launches += 3;
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
+    sh.it_host += 2 * pairs;
+    *ms = (float)(acc / (2.0 * pairs));
+    if (bytes_per_cell) {
+        const bp_config& c = sh.cfg;
+        const double fb = c.precision == BP_PREC_FP32 ? 4 : 3;
+        const double cb = c.precision == BP_PREC_FP32 ? 4 : (c.comp_coef_lo ? 3 : 2);
+        // 2D: the 8 fields read and written once, 7 V + 5 T coefficients read once
+        *bytes_per_cell = 2 * 8 * fb + 12 * cb;
+    }
     return BP_OK;
 }
 

@@ -172,7 +172,8 @@ struct PsiIO {
 // the (phase, axis) slab array; fwd selects the half-grid profile.
 template <int NS, bool RS, class R, bool EX = false>
 __device__ __forceinline__ void cpml_slot(R (&d)[4], void* base, long long cells, int k, cidx sidx,
-                                          bool xaxis, int pos, int x0, const void* pb, const void* pe, R r) {
+                                          bool xaxis, int pos, int x0, const void* pb, const void* pe, R r,
+                                          void* out = nullptr, bool st = true) {
     R* ps = static_cast<R*>(base) + (long long)k * cells + sidx;
     R* pv = static_cast<R*>(base) + (long long)(NS + k) * cells + sidx;
     R psv[4], pvv[4];
@@ -182,8 +183,14 @@ __device__ __forceinline__ void cpml_slot(R (&d)[4], void* base, long long cells
     const R* e = static_cast<const R*>(pe);
     if (xaxis) cpml_x<RS, R, EX>(d, psv, pvv, b, e, x0, r);
     else cpml_s<RS, R, EX>(d, psv, pvv, b[pos], e[pos], r);
-    PsiIO<R>::st(ps, psv);
-    PsiIO<R>::st(pv, pvv);
+    if (out) {       // double-buffered memory variables: the new values go to `out`
+        ps = static_cast<R*>(out) + (long long)k * cells + sidx;
+        pv = static_cast<R*>(out) + (long long)(NS + k) * cells + sidx;
+    }
+    if (st) {
+        PsiIO<R>::st(ps, psv);
+        PsiIO<R>::st(pv, pvv);
+    }
 }
 
 // Slab memory-variable index of a chunk for one axis, or -1 outside the slab.
@@ -211,6 +218,21 @@ __device__ __forceinline__ cidx slab_index(const ShotDesc& S, int axis, int x0, 
 // velocities into V (the marching kernel); otherwise they are loaded here.
 // RS: old state is multiplied by the COMP16 rescale r; the kernels pass false
 // when r is exactly 1, which gives the same bits without the products.
+// Where a phase tail stores: the field arrays (and COMP16 residuals) of the
+// new state, and the memory variables it reads (psi_in) and writes (psi_out).
+// In place, the single-buffered kernels' case, everything is the descriptor's
+// own; the fused step kernel (step_fused.cu) reads one copy of the state and
+// writes the other, and computes without storing on its halo cells.
+struct TailOut {
+    void* const* f;
+    int8_t* const* flo;
+    void* const* psi_in;
+    void* const* psi_out;        // nullptr: in place
+    bool store;                  // false: compute only (the fused kernel's halo cells)
+    __device__ __forceinline__ static TailOut v_of(const ShotDesc& S) { return TailOut{S.f, S.flo, S.psiV, nullptr, true}; }
+    __device__ __forceinline__ static TailOut t_of(const ShotDesc& S) { return TailOut{S.f, S.flo, S.psiT, nullptr, true}; }
+};
+
 template <class R>
 struct VState {
     R x1[4], x3[4], s1[4], z1[4], z2[4], s3[4];       // derivatives (2D and 3D)
@@ -219,9 +241,11 @@ struct VState {
     R rho_y[4], c1_y[4], c2_y[4], vu_y[4], vw_y[4];
 };
 
+// On return V's old-velocity members (vu_*, vw_*) hold the new velocities as a
+// later load of the stored values returns them.
 template <int DIM, int ORD, class P, bool PRE, bool RS, bool NC = kReadOnlyPath>
 __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y, int z, typename P::real r,
-                                       unsigned mask, VState<typename P::real>& V) {
+                                       unsigned mask, VState<typename P::real>& V, const TailOut& O) {
     using R = typename P::real;
     auto &x1 = V.x1, &x3 = V.x3, &s1 = V.s1, &z1 = V.z1, &z2 = V.z2, &s3 = V.s3;
     auto &x2 = V.x2, &y1 = V.y1, &y2 = V.y2, &y3 = V.y3, &s2 = V.s2, &z3 = V.z3;
@@ -254,32 +278,35 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y,
         constexpr int NS = DIM == 3 ? 4 : 3;
         cidx si = slab_index(S, 0, x0, y, z);
         if (si >= 0) {
-            void* B = S.psiV[0];
+            void* B = O.psi_in[0];
+            void* Bo = O.psi_out ? O.psi_out[0] : nullptr;
             const long long n = S.slab_cells[0];
-            cpml_slot<NS, RS, R, P::exact>(x1, B, n, 0, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            cpml_slot<NS, RS, R, P::exact>(s1, B, n, 1, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            cpml_slot<NS, RS, R, P::exact>(z2, B, n, 2, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(y2, B, n, 3, si, true, x0, x0, S.pb[0], S.pe[0], r);
+            cpml_slot<NS, RS, R, P::exact>(x1, B, n, 0, si, true, x0, x0, S.pb2[0], S.pe2[0], r, Bo, O.store);
+            cpml_slot<NS, RS, R, P::exact>(s1, B, n, 1, si, true, x0, x0, S.pb2[0], S.pe2[0], r, Bo, O.store);
+            cpml_slot<NS, RS, R, P::exact>(z2, B, n, 2, si, true, x0, x0, S.pb[0], S.pe[0], r, Bo, O.store);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(y2, B, n, 3, si, true, x0, x0, S.pb[0], S.pe[0], r, Bo, O.store);
         }
         if constexpr (DIM == 3) {
             si = slab_index(S, 1, x0, y, z);
             if (si >= 0) {
-                void* B = S.psiV[1];
+                void* B = O.psi_in[1];
+                void* Bo = O.psi_out ? O.psi_out[1] : nullptr;
                 const long long n = S.slab_cells[1];
-                cpml_slot<NS, RS, R, P::exact>(x2, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, RS, R, P::exact>(y1, B, n, 1, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, RS, R, P::exact>(s2, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, RS, R, P::exact>(z3, B, n, 3, si, false, y, x0, S.pb[1], S.pe[1], r);
+                cpml_slot<NS, RS, R, P::exact>(x2, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r, Bo, O.store);
+                cpml_slot<NS, RS, R, P::exact>(y1, B, n, 1, si, false, y, x0, S.pb2[1], S.pe2[1], r, Bo, O.store);
+                cpml_slot<NS, RS, R, P::exact>(s2, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r, Bo, O.store);
+                cpml_slot<NS, RS, R, P::exact>(z3, B, n, 3, si, false, y, x0, S.pb[1], S.pe[1], r, Bo, O.store);
             }
         }
         si = slab_index(S, 2, x0, y, z);
         if (si >= 0) {
-            void* B = S.psiV[2];
+            void* B = O.psi_in[2];
+            void* Bo = O.psi_out ? O.psi_out[2] : nullptr;
             const long long n = S.slab_cells[2];
-            cpml_slot<NS, RS, R, P::exact>(x3, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, RS, R, P::exact>(z1, B, n, 1, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            cpml_slot<NS, RS, R, P::exact>(s3, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(y3, B, n, 3, si, false, z, x0, S.pb[2], S.pe[2], r);
+            cpml_slot<NS, RS, R, P::exact>(x3, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r, Bo, O.store);
+            cpml_slot<NS, RS, R, P::exact>(z1, B, n, 1, si, false, z, x0, S.pb2[2], S.pe2[2], r, Bo, O.store);
+            cpml_slot<NS, RS, R, P::exact>(s3, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r, Bo, O.store);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(y3, B, n, 3, si, false, z, x0, S.pb[2], S.pe[2], r, Bo, O.store);
         }
     }
 
@@ -299,7 +326,7 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y,
 
     // ---- velocity updates per axis (Float/main.cu:106-113,160-190) ----
     auto axis_update = [&](const R (&sum)[4], const R (&dp)[4], int fu, int fw, const R (&rho)[4],
-                           const R (&c1)[4], const R (&c2)[4], const R (&vu)[4], const R (&vw)[4]) {
+                           const R (&c1)[4], const R (&c2)[4], R (&vu)[4], R (&vw)[4]) {
         R nu[4], nw[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
@@ -323,8 +350,10 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y,
             }
             if (!(mask >> j & 1u)) { nw[j] = vw[j]; nu[j] = vu[j]; }
         }
-        P::st4(S.f[fw], S.flo[fw], c, nw);
-        P::st4(S.f[fu], S.flo[fu], c, nu);
+        P::st4_rt(O.f[fw], O.flo[fw], c, nw, O.store);
+        P::st4_rt(O.f[fu], O.flo[fu], c, nu, O.store);
+#pragma unroll
+        for (int j = 0; j < 4; j++) { vw[j] = nw[j]; vu[j] = nu[j]; }
     };
     if constexpr (!PRE) {
         P::template ld4<NC>(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, rf);
@@ -337,6 +366,12 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y,
     }
     if constexpr (!PRE) load_axis(BP_F_VUZ, BP_F_VWZ, VC_RHO_Z, VC_CC1_Z, VC_CC2_Z, rho_z, c1_z, c2_z, vu_z, vw_z);
     axis_update(sumz, s3, BP_F_VUZ, BP_F_VWZ, rho_z, c1_z, c2_z, vu_z, vw_z);
+}
+
+template <int DIM, int ORD, class P, bool PRE, bool RS, bool NC = kReadOnlyPath>
+__device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y, int z, typename P::real r,
+                                       unsigned mask, VState<typename P::real>& V) {
+    v_tail<DIM, ORD, P, PRE, RS, NC>(S, c, x0, y, z, r, mask, V, TailOut::v_of(S));
 }
 
 // ---------------------------------------------------------------------------
@@ -352,9 +387,10 @@ struct TState {
     R mxy[4], myz[4], oyy[4], oxy[4], oyz[4];
 };
 
+// On return T's old-stress members (op, oxx, ...) hold the new values.
 template <int DIM, int ORD, class P, bool PRE, bool RS, bool NC = kReadOnlyPath>
 __device__ __forceinline__ void t_tail(const ShotDesc& S, cidx c, int x0, int y, int z, typename P::real r,
-                                       unsigned mask, TState<typename P::real>& T) {
+                                       unsigned mask, TState<typename P::real>& T, const TailOut& O) {
     using R = typename P::real;
     auto &uxx = T.uxx, &uzz = T.uzz, &wx = T.wx, &wz = T.wz, &uxz = T.uxz, &uzx = T.uzx;
     auto &uyy = T.uyy, &wy = T.wy, &uxy = T.uxy, &uyx = T.uyx, &uyz = T.uyz, &uzy = T.uzy;
@@ -396,43 +432,45 @@ __device__ __forceinline__ void t_tail(const ShotDesc& S, cidx c, int x0, int y,
         constexpr int NS = DIM == 3 ? 4 : 3;
         cidx si = slab_index(S, 0, x0, y, z);
         if (si >= 0) {
-            void* B = S.psiT[0];
+            void* B = O.psi_in[0];
             const long long n = S.slab_cells[0];
-            cpml_slot<NS, RS, R, P::exact>(uxx, B, n, 0, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            cpml_slot<NS, RS, R, P::exact>(wx, B, n, 1, si, true, x0, x0, S.pb[0], S.pe[0], r);
-            cpml_slot<NS, RS, R, P::exact>(uzx, B, n, 2, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
-            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(uyx, B, n, 3, si, true, x0, x0, S.pb2[0], S.pe2[0], r);
+            cpml_slot<NS, RS, R, P::exact>(uxx, B, n, 0, si, true, x0, x0, S.pb[0], S.pe[0], r, nullptr, O.store);
+            cpml_slot<NS, RS, R, P::exact>(wx, B, n, 1, si, true, x0, x0, S.pb[0], S.pe[0], r, nullptr, O.store);
+            cpml_slot<NS, RS, R, P::exact>(uzx, B, n, 2, si, true, x0, x0, S.pb2[0], S.pe2[0], r, nullptr, O.store);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(uyx, B, n, 3, si, true, x0, x0, S.pb2[0], S.pe2[0], r, nullptr, O.store);
         }
         if constexpr (DIM == 3) {
             si = slab_index(S, 1, x0, y, z);
             if (si >= 0) {
-                void* B = S.psiT[1];
+                void* B = O.psi_in[1];
                 const long long n = S.slab_cells[1];
-                cpml_slot<NS, RS, R, P::exact>(uyy, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, RS, R, P::exact>(wy, B, n, 1, si, false, y, x0, S.pb[1], S.pe[1], r);
-                cpml_slot<NS, RS, R, P::exact>(uxy, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r);
-                cpml_slot<NS, RS, R, P::exact>(uzy, B, n, 3, si, false, y, x0, S.pb2[1], S.pe2[1], r);
+                cpml_slot<NS, RS, R, P::exact>(uyy, B, n, 0, si, false, y, x0, S.pb[1], S.pe[1], r, nullptr, O.store);
+                cpml_slot<NS, RS, R, P::exact>(wy, B, n, 1, si, false, y, x0, S.pb[1], S.pe[1], r, nullptr, O.store);
+                cpml_slot<NS, RS, R, P::exact>(uxy, B, n, 2, si, false, y, x0, S.pb2[1], S.pe2[1], r, nullptr, O.store);
+                cpml_slot<NS, RS, R, P::exact>(uzy, B, n, 3, si, false, y, x0, S.pb2[1], S.pe2[1], r, nullptr, O.store);
             }
         }
         si = slab_index(S, 2, x0, y, z);
         if (si >= 0) {
-            void* B = S.psiT[2];
+            void* B = O.psi_in[2];
             const long long n = S.slab_cells[2];
-            cpml_slot<NS, RS, R, P::exact>(uzz, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, RS, R, P::exact>(wz, B, n, 1, si, false, z, x0, S.pb[2], S.pe[2], r);
-            cpml_slot<NS, RS, R, P::exact>(uxz, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r);
-            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(uyz, B, n, 3, si, false, z, x0, S.pb2[2], S.pe2[2], r);
+            cpml_slot<NS, RS, R, P::exact>(uzz, B, n, 0, si, false, z, x0, S.pb[2], S.pe[2], r, nullptr, O.store);
+            cpml_slot<NS, RS, R, P::exact>(wz, B, n, 1, si, false, z, x0, S.pb[2], S.pe[2], r, nullptr, O.store);
+            cpml_slot<NS, RS, R, P::exact>(uxz, B, n, 2, si, false, z, x0, S.pb2[2], S.pe2[2], r, nullptr, O.store);
+            if constexpr (DIM == 3) cpml_slot<NS, RS, R, P::exact>(uyz, B, n, 3, si, false, z, x0, S.pb2[2], S.pe2[2], r, nullptr, O.store);
         }
     }
 
     // ---- pressure and stress updates (Float/main.cu:287-293) ----
     if constexpr (!PRE) load_state();
     const R dt = S.dtr<R>();
-    auto finish = [&](int f, R (&nv)[4], const R (&ov)[4]) {
+    auto finish = [&](int f, R (&nv)[4], R (&ov)[4]) {
 #pragma unroll
         for (int j = 0; j < 4; j++)
             if (!(mask >> j & 1u)) nv[j] = ov[j];
-        P::st4(S.f[f], S.flo[f], c, nv);
+        if (O.store) P::st4(O.f[f], O.flo[f], c, nv);
+#pragma unroll
+        for (int j = 0; j < 4; j++) ov[j] = nv[j];
     };
     R n[4];
     if constexpr (DIM == 3) {
@@ -518,6 +556,12 @@ __device__ __forceinline__ void t_tail(const ShotDesc& S, cidx c, int x0, int y,
         }
         finish(BP_F_TXZ, n, oxz);
     }
+}
+
+template <int DIM, int ORD, class P, bool PRE, bool RS, bool NC = kReadOnlyPath>
+__device__ __forceinline__ void t_tail(const ShotDesc& S, cidx c, int x0, int y, int z, typename P::real r,
+                                       unsigned mask, TState<typename P::real>& T) {
+    t_tail<DIM, ORD, P, PRE, RS, NC>(S, c, x0, y, z, r, mask, T, TailOut::t_of(S));
 }
 
 }  // namespace bpk

@@ -15,8 +15,8 @@
 // Neighbour rows (y, z) are re-read through L1/L2; DRAM sees each array once
 // per phase.  The CPML memory variables exist on the slabs only; a chunk
 // touches them only when it lies in a slab of that axis.
+#include "post.cuh"
 #include "shot.h"
-#include "stencil.cuh"
 
 namespace bpk {
 
@@ -636,8 +636,6 @@ __device__ __forceinline__ void t_chunk_g(const ShotDesc& S, int x0, int y, int 
 
 // ---------------------------------------------------------------------------
 // Tile loop shared by both phases.
-template <int DIM, class P>
-__device__ __forceinline__ void post_chunk(const ShotDesc& S, int it, cidx c, int x0, int y, int z);
 
 // post (T phase only): each chunk also records the receivers in its cells and,
 // if it holds the source cell, injects the next source sample, in place of the
@@ -760,59 +758,6 @@ __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHAS
 // records the source cell, if any, injects after its own reads; otherwise
 // thread 0 of the shot's first block does.
 template <class P>
-__device__ __forceinline__ typename P::real read_phys(const ShotDesc& S, int f, long long i, typename P::real sc) {
-    return P::ld1(S.f[f], S.flo[f], i) * sc;
-}
-
-template <class P>
-__device__ __forceinline__ void inject(const ShotDesc& S, int it) {
-    using R = typename P::real;
-    if (!S.src_idx_valid || it >= S.nt) return;
-    const long long i = S.src_idx;
-    R I;
-    if constexpr (P::prec == BP_PREC_FP64) I = static_cast<const double*>(S.wavelet)[it];
-    else I = static_cast<const float*>(S.wavelet)[it];
-    // COMP16: the sample enters at the scale the state has when it is added
-    // (that of step it-1); step it's rescale factor then carries it to dyn[it].
-    if constexpr (P::prec == BP_PREC_COMP16) I = I * S.inj_scale * (it > 0 ? S.dyn[it - 1] : 1.0f);
-    if (S.src_mask & BP_SRC_TAU) {
-        P::st1(S.f[BP_F_TXX], S.flo[BP_F_TXX], i, P::ld1(S.f[BP_F_TXX], S.flo[BP_F_TXX], i) + I);
-        if (S.dim == 3) P::st1(S.f[BP_F_TYY], S.flo[BP_F_TYY], i, P::ld1(S.f[BP_F_TYY], S.flo[BP_F_TYY], i) + I);
-        P::st1(S.f[BP_F_TZZ], S.flo[BP_F_TZZ], i, P::ld1(S.f[BP_F_TZZ], S.flo[BP_F_TZZ], i) + I);
-    }
-    if (S.src_mask & BP_SRC_P) P::st1(S.f[BP_F_P], S.flo[BP_F_P], i, P::ld1(S.f[BP_F_P], S.flo[BP_F_P], i) - I);
-}
-
-// Records step it's five components at unique receiver r, cell i.
-template <class P>
-__device__ __forceinline__ void record(const ShotDesc& S, int it, int r, long long i) {
-    using R = typename P::real;
-    R ss = (R)1, sv = (R)1;
-    if constexpr (P::prec == BP_PREC_COMP16) {
-        const float d = 1.0f / S.dyn[it];
-        ss = S.out_stress * d;
-        sv = S.out_vel * d;
-    }
-    R v[BP_NTRACE];
-    v[BP_TR_TXX] = read_phys<P>(S, BP_F_TXX, i, ss);
-    v[BP_TR_TZZ] = read_phys<P>(S, BP_F_TZZ, i, ss);
-    v[BP_TR_VUX] = read_phys<P>(S, BP_F_VUX, i, sv);
-    v[BP_TR_VWX] = read_phys<P>(S, BP_F_VWX, i, sv);
-    v[BP_TR_P] = read_phys<P>(S, BP_F_P, i, ss);
-    const long long cs = (long long)S.nrec * S.nt;
-    bool finite = true;
-#pragma unroll
-    for (int q = 0; q < BP_NTRACE; q++) {
-        S.traces[q * cs + (long long)r * S.nt + it] = (float)v[q];
-        if constexpr (P::prec == BP_PREC_FP64) S.traces64[q * cs + (long long)r * S.nt + it] = v[q];
-        finite = finite && isfinite(v[q]);
-    }
-    // blow-up detection: the first step whose recorded values are not all
-    // finite (step + 1; 0 = none), read by the host at its next sync
-    if (!finite) atomicCAS(S.blowup, 0, it + 1);
-}
-
-template <class P>
 __global__ void k_post(const ShotDesc* __restrict__ shots, int k, int do_record) {
     const ShotDesc& S = shots[blockIdx.y];
     const int it = *S.step_base + k;
@@ -823,39 +768,6 @@ __global__ void k_post(const ShotDesc* __restrict__ shots, int k, int do_record)
     if (owner) inject<P>(S, it + 1);
 }
 
-// k_post's work for the cells of one T-phase chunk (c = flat index of cell
-// x0), after the chunk's stores: the chunk's receivers, found by a binary
-// search of its row's x-sorted list, read back the values this thread has just
-// written (the velocities are not written in the T phase), so the recorded
-// values are k_post's; then the source, if its cell is here.  The receiver on
-// the source cell, if any, is recorded before the injection, as in k_post.
-// The recording and injection, out of line: only the few chunks that hold a
-// receiver or the source call it, and the phase kernels keep their registers.
-template <class P>
-__device__ __noinline__ void post_cells(const ShotDesc& S, int it, cidx c, int x0, int lo, int end) {
-    if (lo < end) {
-        int hi = end;
-        while (lo < hi) {                       // first receiver with x >= x0
-            const int mid = (lo + hi) >> 1;
-            if (S.rec_xu[mid].x < x0) lo = mid + 1;
-            else hi = mid;
-        }
-        for (; lo < end; lo++) {
-            const int2 xu = S.rec_xu[lo];
-            if (xu.x >= x0 + 4) break;
-            record<P>(S, it, xu.y, (long long)c + (xu.x - x0));
-        }
-    }
-    if (S.src_idx_valid && S.src_idx >= c && S.src_idx < (long long)c + 4) inject<P>(S, it + 1);
-}
-
-template <int DIM, class P>
-__device__ __forceinline__ void post_chunk(const ShotDesc& S, int it, cidx c, int x0, int y, int z) {
-    const int key = DIM == 3 ? z * S.ny + y : z;
-    const int lo = S.rec_row[key], end = S.rec_row[key + 1];
-    const bool src = S.src_idx_valid && S.src_idx >= c && S.src_idx < (long long)c + 4;
-    if (lo < end || src) post_cells<P>(S, it, c, x0, lo, end);
-}
 
 // Injection of step it = *step_base + k alone (before the first step).
 template <class P>

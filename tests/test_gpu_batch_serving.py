@@ -136,7 +136,8 @@ def test_every_tile_shape_gives_the_single_shot_results_2d(prec):
     shots = config3_shots(seed=11, nshots=3, nt=120, precision=prec, scale=0.07)
     singles = [alone(c, m) for c, m in shots]
     for shape in SHAPES_2D:
-        b = Batch([c for c, _ in shots], [m for _, m in shots], steps_per_sync=16, ctas_per_sm=2, tile=shape)
+        b = Batch([c for c, _ in shots], [m for _, m in shots], steps_per_sync=16, ctas_per_sm=2, tile=shape,
+                  kernel="register")
         b.run(120)
         b.sync()
         t = b.tune()
@@ -153,7 +154,7 @@ def test_every_tile_shape_gives_the_single_shot_results_3d(prec):
         singles = [alone(c, m) for c, m in order_shots]
         for shape in SHAPES_3D:
             b = Batch([c for c, _ in order_shots], [m for _, m in order_shots], steps_per_sync=16, ctas_per_sm=2,
-                      tile=shape)
+                      tile=shape, kernel="register")
             b.run(90)
             b.sync()
             t = b.tune()
@@ -184,3 +185,21 @@ def test_batch_rejects_a_bad_tile_shape():
         with pytest.raises(BiotError) as e:
             Batch([c for c, _ in shots], [m for _, m in shots], tile=bad)
         assert e.value.code == BP_ERR_ARG
+
+
+@pytest.mark.parametrize("prec", ["fp32", "comp16"])
+def test_fused_kernel_batch_equals_single_shots(prec):
+    """The fused step kernel over a batch of shots of different sizes and
+    lengths (tasks of every shot in one launch): bit-identical to single runs."""
+    shots = config3_shots(seed=14, nshots=4, nt=150, precision=prec, scale=0.09)
+    shots[2][0].nt = 67                     # finishes mid-chunk, on an odd step
+    singles = [alone(c, m) for c, m in shots]
+    b = Batch([c for c, _ in shots], [m for _, m in shots], steps_per_sync=32, ctas_per_sm=0, tile=(8, 1),
+              kernel="fused")
+    assert b.tune()["kernel"] == "fused"
+    b.run(150)
+    b.sync()
+    for i, (tx, tp) in enumerate(singles):
+        assert np.array_equal(b.traces(i, "txx"), tx), i
+        assert np.array_equal(b.traces(i, "p"), tp), i
+    b.close()
