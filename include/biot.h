@@ -45,6 +45,10 @@ extern "C" {
 #define BP_PREC_FP32 0      /* fp32 storage and arithmetic (the Float build)  */
 #define BP_PREC_COMP16 1    /* fp16 hi + int8 residual storage, fp32 math     */
 #define BP_PREC_FP64 2      /* fp64 storage and arithmetic (accuracy reference) */
+#define BP_PREC_CBF16 3     /* compensated bf16 storage: bf16 hi + an unsigned 8-bit
+                               residual = the top 24 bits of the fp32 word (rounded
+                               to nearest even), fp32 arithmetic as BP_PREC_FP32; no
+                               exponent scaling or rescale (bf16 has fp32's range) */
 
 /* FP32 rounding (bp_config.rounding).  FAST divides by H with a reciprocal and
  * one residual step (within one ulp of the IEEE quotient) and forms the CPML

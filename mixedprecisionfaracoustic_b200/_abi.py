@@ -15,7 +15,7 @@ BP_OK = 0
 BP_ERR_ARG, BP_ERR_OOM, BP_ERR_CUDA, BP_ERR_CFL, BP_ERR_UNSTABLE = 1, 2, 3, 4, 5
 BP_ERR_TIMEOUT, BP_ERR_STATE, BP_ERR_NOT_FOUND, BP_ERR_NO_DEVICE, BP_ERR_BUDGET = 6, 7, 8, 9, 10
 
-PREC = {"fp32": 0, "comp16": 1, "fp64": 2}
+PREC = {"fp32": 0, "comp16": 1, "fp64": 2, "cbf16": 3}
 FIELDS = ["vux", "vuy", "vuz", "vwx", "vwy", "vwz", "p", "txx", "tyy", "tzz", "txy", "txz", "tyz"]
 FIELD = {n: i for i, n in enumerate(FIELDS)}
 TRACES = ["txx", "tzz", "vux", "vwx", "p"]          # sisx sisz sisvu sisvw sisp

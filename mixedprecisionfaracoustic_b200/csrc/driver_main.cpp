@@ -1,7 +1,7 @@
 // driver_main.cpp - drop-in for the reference program's main()
 // (Float/main.cu:300-1477 and Half/main.cu:376-1852).
 //
-//   biot_reference_run [--precision fp32|comp16|fp64] [--nt N] [--out DIR]
+//   biot_reference_run [--precision fp32|comp16|cbf16|fp64] [--nt N] [--out DIR]
 //                      [--n NX NY NZ] [--np NP]
 //
 // Same model (create_model: borehole in a porous formation), same grid
@@ -30,12 +30,12 @@ int main(int argc, char** argv) {
         std::string a = argv[i];
         if (a == "--precision" && i + 1 < argc) {
             std::string p = argv[++i];
-            prec = p == "comp16" ? BP_PREC_COMP16 : (p == "fp64" ? BP_PREC_FP64 : BP_PREC_FP32);
+            prec = p == "comp16" ? BP_PREC_COMP16 : (p == "fp64" ? BP_PREC_FP64 : (p == "cbf16" ? BP_PREC_CBF16 : BP_PREC_FP32));
         } else if (a == "--nt" && i + 1 < argc) NT = atoi(argv[++i]);
         else if (a == "--out" && i + 1 < argc) out = argv[++i];
         else if (a == "--np" && i + 1 < argc) NP = atoi(argv[++i]);
         else if (a == "--n" && i + 3 < argc) { NX = atoi(argv[++i]); NY = atoi(argv[++i]); NZ = atoi(argv[++i]); }
-        else { fprintf(stderr, "usage: %s [--precision fp32|comp16|fp64] [--nt N] [--out DIR] [--n NX NY NZ] [--np NP]\n", argv[0]); return 2; }
+        else { fprintf(stderr, "usage: %s [--precision fp32|comp16|cbf16|fp64] [--nt N] [--out DIR] [--n NX NY NZ] [--np NP]\n", argv[0]); return 2; }
     }
     auto t0 = std::chrono::steady_clock::now();
     const int NXe = NX + 2 * NP, NYe = NY + 2 * NP, NZe = NZ + 2 * NP;

@@ -128,6 +128,8 @@ __device__ __forceinline__ void ref32_cc(float c1, float c2, float rhof, float r
     cc2 = (float)__dsub_rn((double)__fsub_rn(c2, rr), h);
 }
 
+// P: PolF32 stores the float coefficients, PolB24 their compensated-bf16 form.
+template <class P>
 __global__ void k_coefs_ref32(ShotDesc S, MediumDev m, float DT) {
     const long long n = (long long)S.nx * S.ny * S.nz;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
@@ -138,13 +140,13 @@ __global__ void k_coefs_ref32(ShotDesc S, MediumDev m, float DT) {
         const long long i = x + (long long)y * S.pitch + (long long)z * S.plane;
         const bool inner = x >= 1 && x < S.nx - 1 && z >= 1 && z < S.nz - 1 && (S.dim == 2 || (y >= 1 && y < S.ny - 1));
         const float rhof = padf(m, MD_RHOF, x, y, z);
-        float* const* vc = reinterpret_cast<float* const*>(S.vc);
-        float* const* tc = reinterpret_cast<float* const*>(S.tc);
-        vc[VC_RHOF][i] = rhof;
-        tc[TC_C][i] = padf(m, MD_C, x, y, z);
-        tc[TC_M][i] = padf(m, MD_M, x, y, z);
-        tc[TC_H][i] = padf(m, MD_H, x, y, z);
-        tc[TC_H2U][i] = padf(m, MD_H2MU, x, y, z);
+        auto vc = [&](int k, float v) { P::st1(S.vc[k], S.vclo[k], i, v); };
+        auto tc = [&](int k, float v) { P::st1(S.tc[k], S.tclo[k], i, v); };
+        vc(VC_RHOF, rhof);
+        tc(TC_C, padf(m, MD_C, x, y, z));
+        tc(TC_M, padf(m, MD_M, x, y, z));
+        tc(TC_H, padf(m, MD_H, x, y, z));
+        tc(TC_H2U, padf(m, MD_H2MU, x, y, z));
         if (!inner) continue;   // outer cells are never updated: coefficients stay 0
         const int rho_slot[3] = {VC_RHO_X, VC_RHO_Y, VC_RHO_Z};
         const int c1_slot[3] = {VC_CC1_X, VC_CC1_Y, VC_CC1_Z};
@@ -154,15 +156,15 @@ __global__ void k_coefs_ref32(ShotDesc S, MediumDev m, float DT) {
             const Ref32Face f = ref32_face(m, x, y, z, a);
             float cc1, cc2;
             ref32_cc(f.c1, f.c2, rhof, f.rho_x, DT, cc1, cc2);
-            vc[rho_slot[a]][i] = f.rho_x;
-            vc[c1_slot[a]][i] = cc1;
-            vc[c2_slot[a]][i] = cc2;
+            vc(rho_slot[a], f.rho_x);
+            vc(c1_slot[a], cc1);
+            vc(c2_slot[a], cc2);
         }
         const float mu = padf(m, MD_MU, x, y, z);
-        tc[TC_MUXZ][i] = ref_harm4(mu, padf(m, MD_MU, x + 1, y, z), padf(m, MD_MU, x, y, z + 1), padf(m, MD_MU, x + 1, y, z + 1));
+        tc(TC_MUXZ, ref_harm4(mu, padf(m, MD_MU, x + 1, y, z), padf(m, MD_MU, x, y, z + 1), padf(m, MD_MU, x + 1, y, z + 1)));
         if (S.dim == 3) {
-            tc[TC_MUYZ][i] = ref_harm4(mu, padf(m, MD_MU, x, y + 1, z), padf(m, MD_MU, x, y, z + 1), padf(m, MD_MU, x, y + 1, z + 1));
-            tc[TC_MUXY][i] = ref_harm4(mu, padf(m, MD_MU, x + 1, y, z), padf(m, MD_MU, x, y + 1, z), padf(m, MD_MU, x + 1, y + 1, z));
+            tc(TC_MUYZ, ref_harm4(mu, padf(m, MD_MU, x, y + 1, z), padf(m, MD_MU, x, y, z + 1), padf(m, MD_MU, x, y + 1, z + 1)));
+            tc(TC_MUXY, ref_harm4(mu, padf(m, MD_MU, x + 1, y, z), padf(m, MD_MU, x, y + 1, z), padf(m, MD_MU, x + 1, y + 1, z)));
         }
     }
 }
@@ -419,7 +421,7 @@ cudaError_t launch_profile(int prec, int n, int np, float H, double dt, double v
                            void* b2, void* e2, cudaStream_t st) {
     PmlGeom g{n, np, H};
     int grid = (n + 255) / 256;
-    if (prec == BP_PREC_FP32)
+    if (prec == BP_PREC_FP32 || prec == BP_PREC_CBF16)
         k_profile_ref32<<<grid, 256, 0, st>>>(g, (float)dt, (float)v0, (float)rc, (float*)b, (float*)e, (float*)b2,
                                               (float*)e2);
     else if (prec == BP_PREC_FP64)
@@ -435,7 +437,8 @@ cudaError_t launch_coefs(int prec, const ShotDesc& S, const float* const* med, i
     for (int k = 0; k < 9; k++) m.a[k] = med[k];
     m.nx = pnx; m.ny = pny; m.nz = pnz; m.np = np;
     const int grid = 148 * 8;
-    if (prec == BP_PREC_FP32) k_coefs_ref32<<<grid, 256, 0, st>>>(S, m, (float)dt);
+    if (prec == BP_PREC_FP32) k_coefs_ref32<PolF32><<<grid, 256, 0, st>>>(S, m, (float)dt);
+    else if (prec == BP_PREC_CBF16) k_coefs_ref32<PolB24><<<grid, 256, 0, st>>>(S, m, (float)dt);
     else if (prec == BP_PREC_COMP16) k_coefs<PolC16><<<grid, 256, 0, st>>>(S, m, dt, em);
     else k_coefs<PolF64><<<grid, 256, 0, st>>>(S, m, dt, em);
     return cudaGetLastError();

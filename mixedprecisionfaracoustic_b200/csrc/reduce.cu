@@ -99,6 +99,7 @@ cudaError_t launch_energy(int prec, const ShotDesc* d_shots, double* partial, do
     const int nb = reduce_blocks();
     if (prec == BP_PREC_FP32) k_energy<PolF32><<<nb, 256, 0, st>>>(d_shots, partial);
     else if (prec == BP_PREC_COMP16) k_energy<PolC16><<<nb, 256, 0, st>>>(d_shots, partial);
+    else if (prec == BP_PREC_CBF16) k_energy<PolB24><<<nb, 256, 0, st>>>(d_shots, partial);
     else k_energy<PolF64><<<nb, 256, 0, st>>>(d_shots, partial);
     k_finish<1><<<1, 1024, 0, st>>>(partial, nb, out);
     return cudaGetLastError();

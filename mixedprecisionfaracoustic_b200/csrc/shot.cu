@@ -44,7 +44,7 @@ int validate_config(const bp_config* c) {
     if (!c) { set_error("null config"); return BP_ERR_ARG; }
     if (c->dim != 2 && c->dim != 3) { set_error("dim must be 2 or 3"); return BP_ERR_ARG; }
     if (c->order != 2 && c->order != 4) { set_error("order must be 2 or 4"); return BP_ERR_ARG; }
-    if (c->precision < BP_PREC_FP32 || c->precision > BP_PREC_FP64) { set_error("bad precision"); return BP_ERR_ARG; }
+    if (c->precision < BP_PREC_FP32 || c->precision > BP_PREC_CBF16) { set_error("bad precision"); return BP_ERR_ARG; }
     if (c->rounding != BP_ROUND_FAST && c->rounding != BP_ROUND_REFERENCE) { set_error("bad rounding"); return BP_ERR_ARG; }
     if (c->rounding == BP_ROUND_REFERENCE && c->precision != BP_PREC_FP32) {
         set_error("reference rounding applies to FP32 only");
@@ -147,8 +147,8 @@ void make_plan(const bp_config* c, int nurec, Plan& p) {
     p.fe = prec == BP_PREC_FP64 ? 8 : (prec == BP_PREC_FP32 ? 4 : 2);
     p.ce = p.fe;
     p.re = prec == BP_PREC_FP64 ? 8 : 4;
-    p.lo_f = prec == BP_PREC_COMP16;
-    p.lo_c = prec == BP_PREC_COMP16 && c->comp_coef_lo;
+    p.lo_f = prec == BP_PREC_COMP16 || prec == BP_PREC_CBF16;
+    p.lo_c = (prec == BP_PREC_COMP16 && c->comp_coef_lo) || prec == BP_PREC_CBF16;
     p.nurec = nurec;
     int ns_ax[3] = {p.nx, p.ny, p.nz};
     for (int a = 0; a < 3; a++) {
@@ -509,7 +509,7 @@ std::vector<std::pair<void*, size_t>> Shot::state_regions() const {
     for (int f = 0; f < BP_NFIELDS; f++) {
         if (!field_used(dim, f)) continue;
         r.emplace_back(desc.f[f], ncell * fe);
-        if (prec == BP_PREC_COMP16) r.emplace_back(desc.flo[f], ncell);
+        if (prec == BP_PREC_COMP16 || prec == BP_PREC_CBF16) r.emplace_back(desc.flo[f], ncell);
     }
     for (int a = 0; a < 3; a++) {
         if (!desc.psiV[a]) continue;

@@ -499,6 +499,7 @@ int bp_algorithmic_bytes(bp_sim* s, double bpc[2], long long* cells) {
     double fb, cb;
     if (c.precision == BP_PREC_FP64) { fb = 8; cb = 8; }
     else if (c.precision == BP_PREC_FP32) { fb = 4; cb = 4; }
+    else if (c.precision == BP_PREC_CBF16) { fb = 3; cb = 3; }
     else { fb = 3; cb = c.comp_coef_lo ? 3 : 2; }
     if (c.dim == 3) {
         bpc[0] = (7 + 2 * 6) * fb + 10 * cb;
@@ -561,7 +562,7 @@ int bp_profile_fused(bp_sim* s, int nsteps, float* ms, double* bytes_per_cell) {
     if (bytes_per_cell) {
         const bp_config& c = sh.cfg;
         const double fb = c.precision == BP_PREC_FP32 ? 4 : 3;
-        const double cb = c.precision == BP_PREC_FP32 ? 4 : (c.comp_coef_lo ? 3 : 2);
+        const double cb = c.precision == BP_PREC_FP32 ? 4 : ((c.comp_coef_lo || c.precision == BP_PREC_CBF16) ? 3 : 2);
         // 2D: the 8 fields read and written once, 7 V + 5 T coefficients read once
         *bytes_per_cell = 2 * 8 * fb + 12 * cb;
     }

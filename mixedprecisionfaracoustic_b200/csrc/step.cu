@@ -882,6 +882,8 @@ cudaError_t launch_phase(int prec, int dim, int order, bool vphase, const ShotDe
         return Launch<PolF32>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
     if (prec == BP_PREC_COMP16)
         return Launch<PolC16>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
+    if (prec == BP_PREC_CBF16)
+        return Launch<PolB24>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
     return Launch<PolF64>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
 }
 
@@ -890,6 +892,7 @@ cudaError_t launch_post(int prec, const ShotDesc* d_shots, int nshots, int max_r
     dim3 grid((max_rec + 127) / 128 > 0 ? (max_rec + 127) / 128 : 1, nshots);
     if (prec == BP_PREC_FP32) k_post<PolF32><<<grid, 128, 0, st>>>(d_shots, k, do_record);
     else if (prec == BP_PREC_COMP16) k_post<PolC16><<<grid, 128, 0, st>>>(d_shots, k, do_record);
+    else if (prec == BP_PREC_CBF16) k_post<PolB24><<<grid, 128, 0, st>>>(d_shots, k, do_record);
     else k_post<PolF64><<<grid, 128, 0, st>>>(d_shots, k, do_record);
     return cudaGetLastError();
 }
@@ -898,6 +901,7 @@ cudaError_t launch_inject(int prec, const ShotDesc* d_shots, int nshots, int k, 
     int g = (nshots + 127) / 128;
     if (prec == BP_PREC_FP32) k_inject<PolF32><<<g, 128, 0, st>>>(d_shots, nshots, k);
     else if (prec == BP_PREC_COMP16) k_inject<PolC16><<<g, 128, 0, st>>>(d_shots, nshots, k);
+    else if (prec == BP_PREC_CBF16) k_inject<PolB24><<<g, 128, 0, st>>>(d_shots, nshots, k);
     else k_inject<PolF64><<<g, 128, 0, st>>>(d_shots, nshots, k);
     return cudaGetLastError();
 }
@@ -911,6 +915,7 @@ cudaError_t launch_snapshot(int prec, const ShotDesc* d_shots, int shot, int f, 
                             cudaStream_t st) {
     if (prec == BP_PREC_FP32) k_snapshot<PolF32><<<296, 256, 0, st>>>(d_shots, shot, f, slice_y, out, it);
     else if (prec == BP_PREC_COMP16) k_snapshot<PolC16><<<296, 256, 0, st>>>(d_shots, shot, f, slice_y, out, it);
+    else if (prec == BP_PREC_CBF16) k_snapshot<PolB24><<<296, 256, 0, st>>>(d_shots, shot, f, slice_y, out, it);
     else k_snapshot<PolF64><<<296, 256, 0, st>>>(d_shots, shot, f, slice_y, out, it);
     return cudaGetLastError();
 }
@@ -918,6 +923,7 @@ cudaError_t launch_snapshot(int prec, const ShotDesc* d_shots, int shot, int f, 
 cudaError_t launch_field_f64(int prec, const ShotDesc* d_shots, int f, double* out, cudaStream_t st) {
     if (prec == BP_PREC_FP32) k_field_f64<PolF32><<<296, 256, 0, st>>>(d_shots, f, out);
     else if (prec == BP_PREC_COMP16) k_field_f64<PolC16><<<296, 256, 0, st>>>(d_shots, f, out);
+    else if (prec == BP_PREC_CBF16) k_field_f64<PolB24><<<296, 256, 0, st>>>(d_shots, f, out);
     else k_field_f64<PolF64><<<296, 256, 0, st>>>(d_shots, f, out);
     return cudaGetLastError();
 }
@@ -932,6 +938,7 @@ int phase_occupancy(int prec, int dim, int order, bool vphase, int rounding) {
         BPK_FN(PolF32R, 2, 2) BPK_FN(PolF32R, 2, 4) BPK_FN(PolF32R, 3, 2) BPK_FN(PolF32R, 3, 4)
     } else if (prec == BP_PREC_FP32) { BPK_FN(PolF32, 2, 2) BPK_FN(PolF32, 2, 4) BPK_FN(PolF32, 3, 2) BPK_FN(PolF32, 3, 4) }
     else if (prec == BP_PREC_COMP16) { BPK_FN(PolC16, 2, 2) BPK_FN(PolC16, 2, 4) BPK_FN(PolC16, 3, 2) BPK_FN(PolC16, 3, 4) }
+    else if (prec == BP_PREC_CBF16) { BPK_FN(PolB24, 2, 2) BPK_FN(PolB24, 2, 4) BPK_FN(PolB24, 3, 2) BPK_FN(PolB24, 3, 4) }
     else { BPK_FN(PolF64, 2, 2) BPK_FN(PolF64, 2, 4) BPK_FN(PolF64, 3, 2) BPK_FN(PolF64, 3, 4) }
 #undef BPK_FN
     if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kThreads, 0) != cudaSuccess) return 1;
@@ -941,6 +948,7 @@ int phase_occupancy(int prec, int dim, int order, bool vphase, int rounding) {
 cudaError_t launch_coef(int prec, const ShotDesc* d_shots, int which, float* out, cudaStream_t st) {
     if (prec == BP_PREC_FP32) k_coef<PolF32><<<296, 256, 0, st>>>(d_shots, which, out);
     else if (prec == BP_PREC_COMP16) k_coef<PolC16><<<296, 256, 0, st>>>(d_shots, which, out);
+    else if (prec == BP_PREC_CBF16) k_coef<PolB24><<<296, 256, 0, st>>>(d_shots, which, out);
     else k_coef<PolF64><<<296, 256, 0, st>>>(d_shots, which, out);
     return cudaGetLastError();
 }

@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kFThreads, (fused_min_blocks<P>())) k_fused(co
 
 // ---------------------------------------------------------------------------
 bool fused_supported(int prec, int dim) {
-    return dim == 2 && (prec == BP_PREC_FP32 || prec == BP_PREC_COMP16);
+    return dim == 2 && (prec == BP_PREC_FP32 || prec == BP_PREC_COMP16 || prec == BP_PREC_CBF16);
 }
 
 bool fused_default() { return BP_FUSED_DEFAULT != 0; }
@@ -330,6 +330,7 @@ int fused_zseg(long long ncol, int nrows, int sms) {
 int fused_occupancy(int prec, int order) {
     const void* fn = nullptr;
     if (prec == BP_PREC_FP32) fn = order == 2 ? (const void*)k_fused<2, PolF32> : (const void*)k_fused<4, PolF32>;
+    else if (prec == BP_PREC_CBF16) fn = order == 2 ? (const void*)k_fused<2, PolB24> : (const void*)k_fused<4, PolB24>;
     else fn = order == 2 ? (const void*)k_fused<2, PolC16> : (const void*)k_fused<4, PolC16>;
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kFThreads, 0) != cudaSuccess) return 1;
@@ -348,6 +349,9 @@ cudaError_t launch_fused(int prec, int order, const ShotDesc* d, int nshots, lon
     } else if (prec == BP_PREC_COMP16) {
         if (order == 2) BPK_FUSED(PolC16, 2);
         else BPK_FUSED(PolC16, 4);
+    } else if (prec == BP_PREC_CBF16) {
+        if (order == 2) BPK_FUSED(PolB24, 2);
+        else BPK_FUSED(PolB24, 4);
     } else {
         return cudaErrorInvalidValue;
     }

@@ -59,7 +59,8 @@ def test_reference_text_format(ref_run, golden):
 def test_fp32_seismograms_match_reference_run():
     """Full 3500-step drop-in run vs the reference's own sis*.dat (regenerated by
     running the unmodified reference Float program on a B200; tests/golden/
-    float_ref_seismograms.npz keeps 26 of the 192 receiver rows)."""
+    float_ref_seismograms.npz keeps 25 of the 192 receiver rows, every 8th and
+    the source row 52)."""
     from conftest import GOLDEN
     g = np.load(GOLDEN / "float_ref_seismograms.npz")
     rows = g["rows"]
