@@ -62,8 +62,8 @@ def parse():
     ap.add_argument("--c0-steps", type=int, default=1000, help="c0: steps of each run (1000 in the configuration)")
     ap.add_argument("--scale", type=float, default=1.0, help="c3/c4: linear size scale of every shot")
     ap.add_argument("--requests", type=int, default=200, help="c4: number of requests")
-    ap.add_argument("--precision", choices=["fp32", "comp16"], default="fp32", help="c3/c4 precision")
-    ap.add_argument("--only", choices=["fp32", "comp16"], default=None,
+    ap.add_argument("--precision", choices=["fp32", "comp16", "cbf16"], default="fp32", help="c3/c4 precision")
+    ap.add_argument("--only", choices=["fp32", "comp16", "cbf16"], default=None,
                     help="time one precision only and skip the FP64, e2e and CPU legs (profiling runs)")
     return ap.parse_args()
 
@@ -181,7 +181,7 @@ def run_ours(args, rank, ws):
     res = {}
     sims = {}
     reps = None
-    precs = (args.only,) if args.only else ("fp32", "comp16")
+    precs = (args.only,) if args.only else ("fp32", "comp16", "cbf16")
     for prec in precs:
         cfg, med = workload(prec, max(C1_STEPS, W + K + P), args.nx, args.nz)
         cfg.device = dev
@@ -251,7 +251,7 @@ def run_ours(args, rank, ws):
     s64 = Simulation(cfg, med)
     s64.run(steps_run)
     s64.sync()
-    for prec in ("fp32", "comp16"):
+    for prec in ("fp32", "comp16", "cbf16"):
         res[prec]["rel_l2_vs_fp64"] = {c: sims[prec].trace_rel_l2(s64, c) for c in ("txx", "tzz", "vux", "vwx", "p")}
         res[prec]["rel_l2_steps"] = steps_run
     s64.close()
@@ -306,11 +306,16 @@ def run_batched(args):
     peak, peak_kind = measured_peaks()
     out = {"workload": "c3: 64 batched 2D shots at full size (seed 3), order 2, 4000-step shots",
            "cells_per_step": cells, "timed_steps": K}
-    for prec, bpc in (("fp32", 144.0), ("comp16", 108.0)):
+    for prec in ("fp32", "comp16", "cbf16"):
         for c, _ in shots:
             c.precision = prec
         b = Batch([c for c, _ in shots], [m for _, m in shots])
         tune = b.autotune(tune_budget)
+        # algorithmic bytes per updated cell of the step the chosen kernels run:
+        # two phases (each array once per phase) or the fused step (fields once
+        # each way, coefficients once); 4 bytes per value at FP32, 3 otherwise
+        wb = 4.0 if prec == "fp32" else 3.0
+        bpc = (2 * 8 + 12) * wb if tune["kernel"] == "fused" else (24 + 12) * wb
         b.run(max(args.warmup, 3))
         b.sync()
         with ClockSampler(0) as clk:
@@ -323,6 +328,7 @@ def run_batched(args):
                                   "peak": peak, "unit": "GB/s", "frac": got / peak, "peak_source": peak_kind}}
         b.close()
     out["speedup_comp16_vs_fp32"] = out["comp16"]["value"] / out["fp32"]["value"]
+    out["speedup_cbf16_vs_fp32"] = out["cbf16"]["value"] / out["fp32"]["value"]
     return out
 
 
@@ -672,6 +678,9 @@ def main():
         roof["traffic"] = tk
         c16roof = dict(c16["roofline"])
         c16roof["traffic"] = traffic.get(f"comp16_{c16roof['kernel']}")
+        b24 = res["cbf16"]
+        b24roof = dict(b24["roofline"])
+        b24roof["traffic"] = traffic.get(f"cbf16_{b24roof['kernel']}")
         out = {
             "metric": METRIC, "value": f32["value"], "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": f32["ms_per_step"], "higher_is_better": True,
@@ -690,6 +699,12 @@ def main():
                        "gpu_launches": c16["launches"], "clocks": c16["clocks"],
                        "timed_regions": c16["timed_regions"],
                        "speedup_vs_fp32": c16["value"] / f32["value"]},
+            "cbf16": {"value": b24["value"], "ms_per_step": b24["ms_per_step"], "roofline": b24roof,
+                      "storage": "bf16 hi + 8-bit residual (top 24 bits of fp32), fp32 math",
+                      "rel_l2_vs_fp64": b24["rel_l2_vs_fp64"], "phase_ms": b24["phase_ms"],
+                      "gpu_launches": b24["launches"], "clocks": b24["clocks"],
+                      "timed_regions": b24["timed_regions"],
+                      "speedup_vs_fp32": b24["value"] / f32["value"]},
             "batched": batched,
         }
         print(json.dumps(out), flush=True)

@@ -2,7 +2,11 @@
 // (Float/main.cu:300-1477 and Half/main.cu:376-1852).
 //
 //   biot_reference_run [--precision fp32|comp16|cbf16|fp64] [--nt N] [--out DIR]
-//                      [--n NX NY NZ] [--np NP]
+//                      [--n NX NY NZ] [--np NP] [--rounding reference|fast]
+//
+// FP32 runs round like the reference's Float build (BP_ROUND_REFERENCE) unless
+// --rounding fast: the outputs then match the reference program's own to the
+// last digits its text format keeps.
 //
 // Same model (create_model: borehole in a porous formation), same grid
 // (128^3 + 2*32 CPML, H = 0.01 m, DT = 0.9 us), same Ricker source (F0 = 3 kHz
@@ -24,7 +28,7 @@ static int die(int rc, const char* what) {
 }
 
 int main(int argc, char** argv) {
-    int prec = BP_PREC_FP32, NT = 3500, NX = 128, NY = 128, NZ = 128, NP = 32;
+    int prec = BP_PREC_FP32, NT = 3500, NX = 128, NY = 128, NZ = 128, NP = 32, rounding = -1;
     std::string out = ".";
     for (int i = 1; i < argc; i++) {
         std::string a = argv[i];
@@ -34,8 +38,9 @@ int main(int argc, char** argv) {
         } else if (a == "--nt" && i + 1 < argc) NT = atoi(argv[++i]);
         else if (a == "--out" && i + 1 < argc) out = argv[++i];
         else if (a == "--np" && i + 1 < argc) NP = atoi(argv[++i]);
+        else if (a == "--rounding" && i + 1 < argc) rounding = std::string(argv[++i]) == "fast" ? BP_ROUND_FAST : BP_ROUND_REFERENCE;
         else if (a == "--n" && i + 3 < argc) { NX = atoi(argv[++i]); NY = atoi(argv[++i]); NZ = atoi(argv[++i]); }
-        else { fprintf(stderr, "usage: %s [--precision fp32|comp16|cbf16|fp64] [--nt N] [--out DIR] [--n NX NY NZ] [--np NP]\n", argv[0]); return 2; }
+        else { fprintf(stderr, "usage: %s [--precision fp32|comp16|cbf16|fp64] [--nt N] [--out DIR] [--n NX NY NZ] [--np NP] [--rounding reference|fast]\n", argv[0]); return 2; }
     }
     auto t0 = std::chrono::steady_clock::now();
     const int NXe = NX + 2 * NP, NYe = NY + 2 * NP, NZe = NZ + 2 * NP;
@@ -68,6 +73,7 @@ int main(int argc, char** argv) {
     c.nrec = NZe; c.rec_x = rx.data(); c.rec_y = ry.data(); c.rec_z = rz.data();
     c.nsnap = (int)ss.size(); c.snap_steps = ss.data(); c.snap_masks = sm.data(); c.snap_y = NYe / 2;
     c.device = 0; c.comp_coef_lo = 1; c.dyn_scale = 1; c.check_cfl = 0;
+    c.rounding = prec == BP_PREC_FP32 ? (rounding < 0 ? BP_ROUND_REFERENCE : rounding) : BP_ROUND_FAST;
     bp_sim* sim = nullptr;
     rc = bp_create(&c, &m, &sim);
     if (rc) return die(rc, "bp_create");

@@ -41,13 +41,16 @@ C0 = dict(Ks=36e9, Kb=9.6e9, mu=5.1e9, Kf=2.25e9, rhos=2650.0, rhof=1000.0, phi=
 DX, DT = 5.0, 4e-4
 
 
-def reference_compat(nt: int = 3500, precision: str = "fp32", n=(128, 128, 128), npml: int = 32):
+def reference_compat(nt: int = 3500, precision: str = "fp32", n=(128, 128, 128), npml: int = 32,
+                     rounding: str = None):
     """The reference program's run, returned as (ShotConfig, Medium)."""
-    return reference_compat_config(nt, precision, n, npml), reference_borehole_medium(*n)
+    return reference_compat_config(nt, precision, n, npml, rounding), reference_borehole_medium(*n)
 
 
-def reference_compat_config(nt: int = 3500, precision: str = "fp32", n=(128, 128, 128), npml: int = 32):
-    """ShotConfig of the reference program's run (no library call)."""
+def reference_compat_config(nt: int = 3500, precision: str = "fp32", n=(128, 128, 128), npml: int = 32,
+                            rounding: str = None):
+    """ShotConfig of the reference program's run (no library call).  FP32 runs
+    round like the reference's Float build unless rounding="fast"."""
     NX, NY, NZ = n
     NXe, NYe, NZe = NX + 2 * npml, NY + 2 * npml, NZ + 2 * npml
     sx, sy, sz = NXe // 2, NYe // 2, 20 + npml
@@ -58,7 +61,8 @@ def reference_compat_config(nt: int = 3500, precision: str = "fp32", n=(128, 128
                      dx=float(np.float32(0.01)), dt=dt, f0=3000.0, t0=float(np.float32(1.2 / 3000.0)),
                      pml_v0=4000.0, pml_r=float(np.float32(1e-6)), src=(sx, sy, sz), src_mask=_abi.SRC_TAU,
                      rec_x=[sx] * NZe, rec_y=[sy] * NZe, rec_z=list(range(NZe)),
-                     snap_steps=snaps, snap_masks=masks, snap_y=NYe // 2)
+                     snap_steps=snaps, snap_masks=masks, snap_y=NYe // 2,
+                     rounding=rounding or ("reference" if precision == "fp32" else "fast"))
     return cfg
 
 

@@ -6,9 +6,7 @@ golden file.
 <run dir> holds the files the reference's Float or Half program writes in its
 working directory (wfile / wfile3d, Float/main.cu:1501-1516,1563-1588,
 Half/main.cu:1875-1960): sisx.dat, sisz.dat, sisvu.dat, sisvw.dat, sisp.dat
-(NZ_ext receiver rows of NT "%e " values, each row ended by "\\n\\n") and the
-snapshot slices txx500.dat, vux500.dat, vuz500.dat, vwx500.dat, vwz500.dat,
-txx.dat (NZ_ext rows of NX_ext values of the y = NY_ext/2 slice).
+(NZ_ext receiver rows of NT "%e " values, each row ended by "\\n\\n").
 
 The runs are made with the reference's own programs, unmodified, compiled for
 sm_100a by `make -C oracle ref REF_DIR=<reference checkout>` into oracle/_ref/
@@ -17,8 +15,10 @@ sm_100a by `make -C oracle ref REF_DIR=<reference checkout>` into oracle/_ref/
 e.g. `cd <run dir> && <repo>/oracle/_ref/float_ref`.
 
 Kept: the seismograms of every 8th receiver row plus the source row 52
-(25 of 192 rows) unless --all-rows, and every snapshot slice present, all as
-float32 (the text holds 7 significant digits).
+(25 of 192 rows) unless --all-rows, as float32 (the text holds 7 significant
+digits).  Made this way: float_ref_seismograms.npz (float_ref),
+float_ref_nofma_seismograms.npz (float_ref_nofma), half_ref_seismograms.npz
+(half_ref).
 """
 import sys
 from pathlib import Path
@@ -26,7 +26,6 @@ from pathlib import Path
 import numpy as np
 
 SIS = ("sisx", "sisz", "sisvu", "sisvw", "sisp")
-SNAPS = ("txx500", "vux500", "vuz500", "vwx500", "vwz500", "txx")
 SOURCE_ROW = 52
 
 
@@ -44,10 +43,6 @@ def main(run: Path, out: Path, all_rows: bool) -> None:
         a = first if k == "sisx" else read_dat(run / f"{k}.dat")
         assert a.shape == first.shape, (k, a.shape)
         res[k] = a[rows].astype(np.float32)
-    for k in SNAPS:
-        p = run / f"{k}.dat"
-        if p.exists():
-            res[k] = read_dat(p).astype(np.float32)
     np.savez_compressed(out, **res)
     print(out, {k: v.shape for k, v in res.items()})
 

@@ -56,39 +56,65 @@ def test_reference_text_format(ref_run, golden):
     assert sis.shape == (192, 501)
 
 
+def _reference_run_traces(precision, rounding=None):
+    from conftest import GOLDEN
+    rows = np.load(GOLDEN / "float_ref_seismograms.npz")["rows"]
+    cfg, med = reference_compat(nt=3500, precision=precision, rounding=rounding)
+    with Simulation(cfg, med) as s:
+        s.run(3500)
+        return {k: s.traces(c)[rows].astype(np.float64) for k, c in COMPS}
+
+
+COMPS = (("sisx", "txx"), ("sisz", "tzz"), ("sisvu", "vux"), ("sisvw", "vwx"), ("sisp", "p"))
+
+
 def test_fp32_seismograms_match_reference_run():
     """Full 3500-step drop-in run vs the reference's own sis*.dat (regenerated by
-    running the unmodified reference Float program on a B200; tests/golden/
-    float_ref_seismograms.npz keeps 25 of the 192 receiver rows, every 8th and
-    the source row 52)."""
+    running the unmodified reference Float program on a B200;
+    tests/golden/float_ref_seismograms.npz keeps 25 of the 192 receiver rows,
+    every 8th and the source row 52).
+
+    With the reference's rounding (the drop-in's default for FP32) every
+    component matches to <= 1e-6 over all steps (measured <= 1.5e-7, the text
+    files' own 7-digit rounding).  The fast rounding is held to the FP64
+    solution instead: sisvu's late coda is at float noise level, and the
+    reference itself moves by 1.3e-5 on sisvu when it is only recompiled
+    without FMA contraction (test_oracle_golden.py); the fast form is closer
+    to FP64 than the reference on sisvu and within 1e-5 of it elsewhere."""
     from conftest import GOLDEN
     g = np.load(GOLDEN / "float_ref_seismograms.npz")
-    rows = g["rows"]
-    comps = (("sisx", "txx"), ("sisz", "tzz"), ("sisvu", "vux"), ("sisvw", "vwx"), ("sisp", "p"))
-    got, f64 = {}, {}
-    for prec, out in (("fp32", got), ("fp64", f64)):
-        cfg, med = reference_compat(nt=3500, precision=prec)
-        with Simulation(cfg, med) as s:
-            s.run(3500)
-            out.update({k: s.traces(c)[rows].astype(np.float64) for k, c in comps})
+    ref = _reference_run_traces("fp32", "reference")
+    for k, _ in COMPS:
+        if k == "sisvw":
+            continue
+        err = rel_l2(ref[k], g[k])
+        assert err <= 1e-6, f"reference rounding {k}: rel L2 {err:.3e}"
+    fast = _reference_run_traces("fp32", "fast")
+    f64 = _reference_run_traces("fp64")
     for k in ("sisx", "sisz", "sisp"):
-        err = rel_l2(got[k], g[k])
-        assert err <= 1e-5, f"{k}: rel L2 {err:.3e}"
-    # sisvu's late coda amplifies rounding: the reference's own Float output is
-    # 3.5e-5 away from the FP64 solution on these rows, so two float programs
-    # that round differently (nvcc's FMA contraction choices) cannot agree to
-    # 1e-5 over all 3500 steps.  Required instead: 1e-5 over the first 1000
-    # steps, 5e-5 over the whole run, and the FP32 path at least as close to
-    # the FP64 solution as the reference's Float build is.
-    err_early = rel_l2(got["sisvu"][:, :1000], g["sisvu"][:, :1000])
-    assert err_early <= 1e-5, f"sisvu t<1000: rel L2 {err_early:.3e}"
-    err = rel_l2(got["sisvu"], g["sisvu"])
-    assert err <= 5e-5, f"sisvu: rel L2 {err:.3e}"
-    mine, theirs = rel_l2(got["sisvu"], f64["sisvu"]), rel_l2(g["sisvu"], f64["sisvu"])
+        assert rel_l2(fast[k], g[k]) <= 1e-5, k
+        assert rel_l2(fast[k], f64[k]) <= 1e-5, k
+    mine, theirs = rel_l2(fast["sisvu"], f64["sisvu"]), rel_l2(g["sisvu"], f64["sisvu"])
     assert mine <= theirs, (mine, theirs)
+    assert np.all(fast["sisvw"] == 0) and np.all(g["sisvw"] == 0)   # receivers in the fluid borehole
+
+
+def test_comp16_as_close_to_fp64_as_the_reference_half_build():
+    """COMP16 (the reference's compensated fp16 storage) over the full 3500-step
+    reference run, against the unmodified reference Half build's own outputs
+    (tests/golden/half_ref_seismograms.npz, same rows): per component, the
+    distance to the FP64 solution is at most 1.5 x the Half build's (measured
+    0.18 x on sisx and sisz, 1.04 x on sisvu, 1.42 x on sisp), and the two
+    agree with each other to <= 3e-4 on the stress traces."""
+    from conftest import GOLDEN
+    h = np.load(GOLDEN / "half_ref_seismograms.npz")
+    c16 = _reference_run_traces("comp16")
+    f64 = _reference_run_traces("fp64")
+    for k in ("sisx", "sisz", "sisvu", "sisp"):
+        mine, theirs = rel_l2(c16[k], f64[k]), rel_l2(h[k], f64[k])
+        assert mine <= 1.5 * theirs and mine <= 1e-3, (k, mine, theirs)
     for k in ("sisx", "sisz", "sisp"):
-        assert rel_l2(got[k], f64[k]) <= 1e-5, k
-    assert np.all(got["sisvw"] == 0) and np.all(g["sisvw"] == 0)   # receivers in the fluid borehole
+        assert rel_l2(c16[k], h[k]) <= 3e-4, k
 
 
 def test_comp16_reference_run_vs_fp64():
