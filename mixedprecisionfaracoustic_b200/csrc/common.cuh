@@ -181,6 +181,7 @@ __device__ __forceinline__ T ldv(const T* p) {
 struct PolF32 {
     using real = float;
     static constexpr int prec = BP_PREC_FP32;
+    static constexpr int store = BP_PREC_FP32;   // storage format (PolB24: BP_PREC_CBF16)
     static constexpr bool exact = false;      // reference rounding (PolF32R)
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
@@ -221,6 +222,7 @@ struct PolF32 {
 struct PolF64 {
     using real = double;
     static constexpr int prec = BP_PREC_FP64;
+    static constexpr int store = BP_PREC_FP64;
     static constexpr bool exact = false;
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
@@ -331,6 +333,7 @@ struct PolB24 : PolF32 {
 struct PolC16 {
     using real = float;
     static constexpr int prec = BP_PREC_COMP16;
+    static constexpr int store = BP_PREC_COMP16;
     static constexpr bool exact = false;
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t* lo, cidx i, real (&v)[4]) {

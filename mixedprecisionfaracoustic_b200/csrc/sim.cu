@@ -454,6 +454,19 @@ int bp_get_scaling(bp_sim* s, int* em, int* es, float* dyn_scale, double* kmax, 
     return BP_OK;
 }
 
+// Per-launch device times from events recorded around every launch of the
+// profiled steps, read after one synchronisation at the end: a wait per step
+// would leave the GPU idle between steps and time each launch from idle.
+struct EventRing {
+    std::vector<cudaEvent_t> ev;
+    ~EventRing() { for (auto e : ev) cudaEventDestroy(e); }
+    cudaError_t make(size_t n) {
+        ev.resize(n, nullptr);
+        for (auto& e : ev) { cudaError_t r = cudaEventCreate(&e); if (r != cudaSuccess) return r; }
+        return cudaSuccess;
+    }
+};
+
 int bp_profile_phases(bp_sim* s, int nsteps, float ms[3]) {
     if (!s || !ms || nsteps < 1) { set_error("bad arguments"); return BP_ERR_ARG; }
     SIM_CK(cudaSetDevice(s->device));
@@ -461,11 +474,11 @@ int bp_profile_phases(bp_sim* s, int nsteps, float ms[3]) {
     Runner& R = s->run;
     nsteps = std::min(nsteps, sh.cfg.nt - sh.it_host);
     if (nsteps < 1) { set_error("no steps left to profile"); return BP_ERR_STATE; }
-    cudaEvent_t ev[4];
-    for (auto& x : ev) SIM_CK(cudaEventCreate(&x));
-    double acc[3] = {0, 0, 0};
+    EventRing E;
+    SIM_CK(E.make((size_t)4 * nsteps));
     cudaError_t e = cudaSuccess;
     for (int i = 0; i < nsteps && e == cudaSuccess; i++) {
+        cudaEvent_t* ev = &E.ev[4 * i];
         cudaEventRecord(ev[0], s->st);
         e = R.phase(true, 0);
         cudaEventRecord(ev[1], s->st);
@@ -474,16 +487,17 @@ int bp_profile_phases(bp_sim* s, int nsteps, float ms[3]) {
         if (e == cudaSuccess && !R.fused_post()) e = launch_post(R.prec, R.d_shots, R.nshots, R.max_rec, 0, 1, s->st);
         if (e == cudaSuccess) e = launch_advance(R.d_shots, R.nshots, 1, s->st);
         cudaEventRecord(ev[3], s->st);
-        if (e == cudaSuccess) e = cudaEventSynchronize(ev[3]);
-        float t;
-        for (int q = 0; q < 3 && e == cudaSuccess; q++) {
-            cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
-            acc[q] += t;
-        }
         R.launches += R.launches_per_step() + 1;
     }
-    for (auto& x : ev) cudaEventDestroy(x);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
+    double acc[3] = {0, 0, 0};
+    for (int i = 0; i < nsteps; i++)
+        for (int q = 0; q < 3; q++) {
+            float t = 0;
+            cudaEventElapsedTime(&t, E.ev[4 * i + q], E.ev[4 * i + q + 1]);
+            acc[q] += t;
+        }
     sh.it_host += nsteps;
     for (int q = 0; q < 3; q++) ms[q] = (float)(acc[q] / nsteps);
     return BP_OK;
@@ -535,28 +549,28 @@ int bp_profile_fused(bp_sim* s, int nsteps, float* ms, double* bytes_per_cell) {
     SIM_CK(cudaSetDevice(s->device));
     const int pairs = std::min((nsteps + 1) / 2, (sh.cfg.nt - sh.it_host) / 2);
     if (pairs < 1) { set_error("no steps left to profile"); return BP_ERR_STATE; }
-    cudaEvent_t ev[3];
-    for (auto& x : ev) SIM_CK(cudaEventCreate(&x));
-    double acc = 0;
+    EventRing E;
+    SIM_CK(E.make((size_t)3 * pairs));
     cudaError_t e = cudaSuccess;
     for (int i = 0; i < pairs && e == cudaSuccess; i++) {
+        cudaEvent_t* ev = &E.ev[3 * i];
         cudaEventRecord(ev[0], s->st);
         e = launch_fused(R.prec, R.order, R.d_shots, R.nshots, R.ntiles_f, 0, 0, R.grid_f, s->st);
         cudaEventRecord(ev[1], s->st);
         if (e == cudaSuccess) e = launch_fused(R.prec, R.order, R.d_shots, R.nshots, R.ntiles_f, 1, 1, R.grid_f, s->st);
         cudaEventRecord(ev[2], s->st);
         if (e == cudaSuccess) e = launch_advance(R.d_shots, R.nshots, 2, s->st);
-        if (e == cudaSuccess) e = cudaEventSynchronize(ev[2]);
-        float t0 = 0, t1 = 0;
-        if (e == cudaSuccess) {
-            cudaEventElapsedTime(&t0, ev[0], ev[1]);
-            cudaEventElapsedTime(&t1, ev[1], ev[2]);
-            acc += t0 + t1;
-        }
         R.launches += 3;
     }
-    for (auto& x : ev) cudaEventDestroy(x);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return BP_ERR_CUDA; }
+    double acc = 0;
+    for (int i = 0; i < pairs; i++) {
+        float t0 = 0, t1 = 0;
+        cudaEventElapsedTime(&t0, E.ev[3 * i], E.ev[3 * i + 1]);
+        cudaEventElapsedTime(&t1, E.ev[3 * i + 1], E.ev[3 * i + 2]);
+        acc += t0 + t1;
+    }
     sh.it_host += 2 * pairs;
     *ms = (float)(acc / (2.0 * pairs));
     if (bytes_per_cell) {

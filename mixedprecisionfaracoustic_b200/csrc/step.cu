@@ -79,8 +79,20 @@ __device__ __forceinline__ int locate_shot(const ShotDesc* shots, int nshots, lo
 #ifndef BP_MINB3_F64
 #define BP_MINB3_F64 2
 #endif
+// Compensated-BF16 storage (FP32 arithmetic, 3-byte values, a two-instruction
+// decode): its own caps.
+#ifndef BP_MINB_B24
+#define BP_MINB_B24 3
+#endif
+#ifndef BP_MINB_B24_V
+#define BP_MINB_B24_V 3
+#endif
+#ifndef BP_MINB3_B24
+#define BP_MINB3_B24 3
+#endif
 template <int DIM, int ORD, class P, bool VPHASE>
 __host__ __device__ constexpr int phase_min_blocks() {
+    if (P::store == BP_PREC_CBF16) return DIM == 3 ? BP_MINB3_B24 : (VPHASE ? BP_MINB_B24_V : BP_MINB_B24);
     if (DIM == 3) return P::prec == BP_PREC_FP32 ? BP_MINB3_F32 : P::prec == BP_PREC_COMP16 ? BP_MINB3_C16 : BP_MINB3_F64;
     return P::prec == BP_PREC_FP32 ? BP_MINB_F32
                                    : P::prec == BP_PREC_COMP16 ? (VPHASE ? BP_MINB_C16_V : BP_MINB_C16) : BP_MINB_F64;
@@ -116,7 +128,9 @@ __host__ __device__ constexpr bool read_only_loads() {
 
 // ---------------------------------------------------------------------------
 // V phase for one 4-cell chunk: FD_V (Float/main.cu:103-191).
-template <int DIM, int ORD, class P, bool RS>
+// NCOK = false: no read-only-path loads (the interleaved step kernel reads
+// arrays that the same launch writes)
+template <int DIM, int ORD, class P, bool RS, bool NCOK = true>
 __device__ __forceinline__ void v_chunk(const ShotDesc& S, int x0, int y, int z, typename P::real r,
                                         unsigned mask) {
     using R = typename P::real;
@@ -131,63 +145,63 @@ __device__ __forceinline__ void v_chunk(const ShotDesc& S, int x0, int y, int z,
     // ---- derivatives of the old stresses (x1..s3, Float/main.cu:115-128) ----
     {
         R v[4 + ORD];
-        load_span<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_TXX], S.flo[BP_F_TXX], row, x0, S.nx, v);       // txx: D+x
+        load_span<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TXX], S.flo[BP_F_TXX], row, x0, S.nx, v);       // txx: D+x
 #pragma unroll
         for (int j = 0; j < 4; j++) x1[j] = deriv_div<P>(dfwd<ORD>(v, j), S);
-        load_span<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_P], S.flo[BP_F_P], row, x0, S.nx, v);           // p: D+x
+        load_span<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_P], S.flo[BP_F_P], row, x0, S.nx, v);           // p: D+x
 #pragma unroll
         for (int j = 0; j < 4; j++) s1[j] = deriv_div<P>(dfwd<ORD>(v, j), S);
-        load_span<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_TXZ], S.flo[BP_F_TXZ], row, x0, S.nx, v);       // txz: D-x
+        load_span<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TXZ], S.flo[BP_F_TXZ], row, x0, S.nx, v);       // txz: D-x
 #pragma unroll
         for (int j = 0; j < 4; j++) z2[j] = deriv_div<P>(dbwd<ORD>(v, j), S);
         R a[ORD + 1][4];
-        load_rows<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_TXZ], S.flo[BP_F_TXZ], c, sz, a);               // txz: D-z
+        load_rows<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TXZ], S.flo[BP_F_TXZ], c, sz, a);               // txz: D-z
 #pragma unroll
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
             x3[j] = deriv_div<P>(rbwd<ORD>(t), S); }
-        load_rows<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_TZZ], S.flo[BP_F_TZZ], c, sz, a);               // tzz: D+z
+        load_rows<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TZZ], S.flo[BP_F_TZZ], c, sz, a);               // tzz: D+z
 #pragma unroll
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
             z1[j] = deriv_div<P>(rfwd<ORD>(t), S); }
-        load_rows<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_P], S.flo[BP_F_P], c, sz, a);                   // p: D+z
+        load_rows<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_P], S.flo[BP_F_P], c, sz, a);                   // p: D+z
 #pragma unroll
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
             s3[j] = deriv_div<P>(rfwd<ORD>(t), S); }
         if constexpr (DIM == 3) {
-            load_span<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_TXY], S.flo[BP_F_TXY], row, x0, S.nx, v);   // txy: D-x
+            load_span<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TXY], S.flo[BP_F_TXY], row, x0, S.nx, v);   // txy: D-x
 #pragma unroll
             for (int j = 0; j < 4; j++) y2[j] = deriv_div<P>(dbwd<ORD>(v, j), S);
-            load_rows<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_TXY], S.flo[BP_F_TXY], c, sy, a);           // txy: D-y
+            load_rows<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TXY], S.flo[BP_F_TXY], c, sy, a);           // txy: D-y
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
                 for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
                 x2[j] = deriv_div<P>(rbwd<ORD>(t), S); }
-            load_rows<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_TYY], S.flo[BP_F_TYY], c, sy, a);           // tyy: D+y
+            load_rows<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TYY], S.flo[BP_F_TYY], c, sy, a);           // tyy: D+y
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
                 for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
                 y1[j] = deriv_div<P>(rfwd<ORD>(t), S); }
-            load_rows<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_TYZ], S.flo[BP_F_TYZ], c, sz, a);           // tyz: D-z
+            load_rows<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TYZ], S.flo[BP_F_TYZ], c, sz, a);           // tyz: D-z
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
                 for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
                 y3[j] = deriv_div<P>(rbwd<ORD>(t), S); }
-            load_rows<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_TYZ], S.flo[BP_F_TYZ], c, sy, a);           // tyz: D-y
+            load_rows<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TYZ], S.flo[BP_F_TYZ], c, sy, a);           // tyz: D-y
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
                 for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
                 z3[j] = deriv_div<P>(rbwd<ORD>(t), S); }
-            load_rows<ORD, P, read_only_loads<DIM, P, true>()>(S.f[BP_F_P], S.flo[BP_F_P], c, sy, a);               // p: D+y
+            load_rows<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_P], S.flo[BP_F_P], c, sy, a);               // p: D+y
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
@@ -195,12 +209,12 @@ __device__ __forceinline__ void v_chunk(const ShotDesc& S, int x0, int y, int z,
                 s2[j] = deriv_div<P>(rfwd<ORD>(t), S); }
         }
     }
-    v_tail<DIM, ORD, P, false, RS, read_only_loads<DIM, P, true>()>(S, c, x0, y, z, r, mask, V);
+    v_tail<DIM, ORD, P, false, RS, (read_only_loads<DIM, P, true>() && NCOK)>(S, c, x0, y, z, r, mask, V);
 }
 
 // ---------------------------------------------------------------------------
 // T phase for one 4-cell chunk: FD_T (Float/main.cu:232-294).
-template <int DIM, int ORD, class P, bool RS>
+template <int DIM, int ORD, class P, bool RS, bool NCOK = true>
 __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z, typename P::real r,
                                         unsigned mask) {
     using R = typename P::real;
@@ -215,62 +229,62 @@ __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z,
     {
         R v[4 + ORD];
         R a[ORD + 1][4];
-        load_span<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VUX], S.flo[BP_F_VUX], row, x0, S.nx, v);       // vux: D-x
+        load_span<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUX], S.flo[BP_F_VUX], row, x0, S.nx, v);       // vux: D-x
 #pragma unroll
         for (int j = 0; j < 4; j++) uxx[j] = deriv_div<P>(dbwd<ORD>(v, j), S);
-        load_span<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VWX], S.flo[BP_F_VWX], row, x0, S.nx, v);       // vwx: D-x
+        load_span<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VWX], S.flo[BP_F_VWX], row, x0, S.nx, v);       // vwx: D-x
 #pragma unroll
         for (int j = 0; j < 4; j++) wx[j] = deriv_div<P>(dbwd<ORD>(v, j), S);
-        load_span<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VUZ], S.flo[BP_F_VUZ], row, x0, S.nx, v);       // vuz: D+x
+        load_span<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUZ], S.flo[BP_F_VUZ], row, x0, S.nx, v);       // vuz: D+x
 #pragma unroll
         for (int j = 0; j < 4; j++) uzx[j] = deriv_div<P>(dfwd<ORD>(v, j), S);
-        load_rows<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VUZ], S.flo[BP_F_VUZ], c, sz, a);               // vuz: D-z
+        load_rows<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUZ], S.flo[BP_F_VUZ], c, sz, a);               // vuz: D-z
 #pragma unroll
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
             uzz[j] = deriv_div<P>(rbwd<ORD>(t), S); }
-        load_rows<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VWZ], S.flo[BP_F_VWZ], c, sz, a);               // vwz: D-z
+        load_rows<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VWZ], S.flo[BP_F_VWZ], c, sz, a);               // vwz: D-z
 #pragma unroll
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
             wz[j] = deriv_div<P>(rbwd<ORD>(t), S); }
-        load_rows<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VUX], S.flo[BP_F_VUX], c, sz, a);               // vux: D+z
+        load_rows<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUX], S.flo[BP_F_VUX], c, sz, a);               // vux: D+z
 #pragma unroll
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
             uxz[j] = deriv_div<P>(rfwd<ORD>(t), S); }
         if constexpr (DIM == 3) {
-            load_span<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VUY], S.flo[BP_F_VUY], row, x0, S.nx, v);   // vuy: D+x
+            load_span<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUY], S.flo[BP_F_VUY], row, x0, S.nx, v);   // vuy: D+x
 #pragma unroll
             for (int j = 0; j < 4; j++) uyx[j] = deriv_div<P>(dfwd<ORD>(v, j), S);
-            load_rows<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VUY], S.flo[BP_F_VUY], c, sy, a);           // vuy: D-y
+            load_rows<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUY], S.flo[BP_F_VUY], c, sy, a);           // vuy: D-y
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
                 for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
                 uyy[j] = deriv_div<P>(rbwd<ORD>(t), S); }
-            load_rows<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VWY], S.flo[BP_F_VWY], c, sy, a);           // vwy: D-y
+            load_rows<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VWY], S.flo[BP_F_VWY], c, sy, a);           // vwy: D-y
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
                 for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
                 wy[j] = deriv_div<P>(rbwd<ORD>(t), S); }
-            load_rows<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VUX], S.flo[BP_F_VUX], c, sy, a);           // vux: D+y
+            load_rows<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUX], S.flo[BP_F_VUX], c, sy, a);           // vux: D+y
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
                 for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
                 uxy[j] = deriv_div<P>(rfwd<ORD>(t), S); }
-            load_rows<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VUY], S.flo[BP_F_VUY], c, sz, a);           // vuy: D+z
+            load_rows<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUY], S.flo[BP_F_VUY], c, sz, a);           // vuy: D+z
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
                 for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
                 uyz[j] = deriv_div<P>(rfwd<ORD>(t), S); }
-            load_rows<ORD, P, read_only_loads<DIM, P, false>()>(S.f[BP_F_VUZ], S.flo[BP_F_VUZ], c, sy, a);           // vuz: D+y
+            load_rows<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUZ], S.flo[BP_F_VUZ], c, sy, a);           // vuz: D+y
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
@@ -278,7 +292,7 @@ __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z,
                 uzy[j] = deriv_div<P>(rfwd<ORD>(t), S); }
         }
     }
-    t_tail<DIM, ORD, P, false, RS, read_only_loads<DIM, P, false>()>(S, c, x0, y, z, r, mask, T);
+    t_tail<DIM, ORD, P, false, RS, (read_only_loads<DIM, P, false>() && NCOK)>(S, c, x0, y, z, r, mask, T);
 }
 
 // ---------------------------------------------------------------------------
@@ -635,11 +649,76 @@ __device__ __forceinline__ void t_chunk_g(const ShotDesc& S, int x0, int y, int 
 }
 
 // ---------------------------------------------------------------------------
-// Tile loop shared by both phases.
+// The (row, segment) units of tile (rb, sb) of shot S in one phase (it: the
+// step index, r: the COMP16 rescale factor of that step).  post (T phase
+// only): each chunk also records the receivers in its cells and, if it holds
+// the source cell, injects the next source sample, in place of the post-step
+// kernel k_post.
+template <int DIM, int ORD, class P, bool VPHASE, bool MU, bool NCOK>
+__device__ __forceinline__ void tile_units(const ShotDesc& S, int rb, int sb, int warp, int lane, typename P::real r,
+                                           int it, int post) {
+    using R = typename P::real;
+    // the tile's (row, segment) units, warp w taking units w, w + 8, ...;
+    // consecutive warps take consecutive rows
+    const int lr = S.tile_lr, units = 1 << (lr + S.tile_ls);
+    auto unit = [&](int u) {
+        const int ri = u & ((1 << lr) - 1);
+        const int seg = (sb << S.tile_ls) + (u >> lr);
+        if (seg >= S.nseg) return;
+        int y, z;
+        if constexpr (DIM == 3) {
+            const int ltz = S.tile_ltz, lty = lr - ltz;
+            const int nyb = (S.ny + (1 << lty) - 1) >> lty;
+            const int zb = rb / nyb, yb = rb - zb * nyb;
+            y = (yb << lty) + (ri & ((1 << lty) - 1));
+            z = (zb << ltz) + (ri >> lty);
+            if (y >= S.ny || z >= S.nz) return;
+        } else {
+            const int row = (rb << lr) + ri;
+            if (row >= S.nrows) return;
+            y = 0;
+            z = row;
+        }
+        const int hw = ORD / 2;
+        if (z < hw || z >= S.nz - hw) return;
+        if (DIM == 3 && (y < hw || y >= S.ny - hw)) return;
+        const int x0 = seg * kSegCells + lane * 4;
+        if (x0 >= S.nx - hw || x0 + 3 < hw) return;
+        unsigned mask = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (x0 + j >= hw && x0 + j < S.nx - hw) mask |= 1u << j;
+        // COMP16: the rescale products only on the steps whose factor is not
+        // exactly 1 (a uniform branch; the products are never fused, so both
+        // forms give the same bits when r == 1)
+        if constexpr (grouped<DIM, P, VPHASE>()) {
+            if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
+                if constexpr (VPHASE) v_chunk_g<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+                else t_chunk_g<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
+            } else {
+                if constexpr (VPHASE) v_chunk_g<DIM, ORD, P, false>(S, x0, y, z, r, mask);
+                else t_chunk_g<DIM, ORD, P, false>(S, x0, y, z, r, mask);
+            }
+        } else if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
+            if constexpr (VPHASE) v_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16, NCOK>(S, x0, y, z, r, mask);
+            else t_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16, NCOK>(S, x0, y, z, r, mask);
+        } else {
+            if constexpr (VPHASE) v_chunk<DIM, ORD, P, false, NCOK>(S, x0, y, z, r, mask);
+            else t_chunk<DIM, ORD, P, false, NCOK>(S, x0, y, z, r, mask);
+        }
+        if constexpr (!VPHASE)
+            if (post) post_chunk<DIM, P>(S, it, x0 + y * (cidx)S.pitch + z * (cidx)S.plane, x0, y, z);
+    };
+    // MU: tiles of more units than warps (16-row or 8 x 2 tiles); the
+    // one-unit form keeps no loop state live across the chunk code, which
+    // costs the 2D FP32 V phase its spill-free 80 registers otherwise
+    if constexpr (MU) {
+        for (int u = warp; u < units; u += kWarps) unit(u);
+    } else {
+        if (warp < units) unit(warp);
+    }
+}
 
-// post (T phase only): each chunk also records the receivers in its cells and,
-// if it holds the source cell, injects the next source sample, in place of the
-// post-step kernel k_post.
 template <int DIM, int ORD, class P, bool VPHASE, bool MU>
 __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHASE>())) k_phase(const ShotDesc* __restrict__ shots, int nshots,
                                                      long long ntiles, int k, int post) {
@@ -688,65 +767,7 @@ __global__ void __launch_bounds__(kThreads, (phase_min_blocks<DIM, ORD, P, VPHAS
             rb = (int)(lt / S.nseg_t);
             sb = (int)(lt % S.nseg_t);
         }
-        // the tile's (row, segment) units, warp w taking units w, w + 8, ...;
-        // consecutive warps take consecutive rows
-        const int lr = S.tile_lr, units = 1 << (lr + S.tile_ls);
-        auto unit = [&](int u) {
-            const int ri = u & ((1 << lr) - 1);
-            const int seg = (sb << S.tile_ls) + (u >> lr);
-            if (seg >= S.nseg) return;
-            int y, z;
-            if constexpr (DIM == 3) {
-                const int ltz = S.tile_ltz, lty = lr - ltz;
-                const int nyb = (S.ny + (1 << lty) - 1) >> lty;
-                const int zb = rb / nyb, yb = rb - zb * nyb;
-                y = (yb << lty) + (ri & ((1 << lty) - 1));
-                z = (zb << ltz) + (ri >> lty);
-                if (y >= S.ny || z >= S.nz) return;
-            } else {
-                const int row = (rb << lr) + ri;
-                if (row >= S.nrows) return;
-                y = 0;
-                z = row;
-            }
-            const int hw = ORD / 2;
-            if (z < hw || z >= S.nz - hw) return;
-            if (DIM == 3 && (y < hw || y >= S.ny - hw)) return;
-            const int x0 = seg * kSegCells + lane * 4;
-            if (x0 >= S.nx - hw || x0 + 3 < hw) return;
-            unsigned mask = 0;
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (x0 + j >= hw && x0 + j < S.nx - hw) mask |= 1u << j;
-            // COMP16: the rescale products only on the steps whose factor is not
-            // exactly 1 (a uniform branch; the products are never fused, so both
-            // forms give the same bits when r == 1)
-            if constexpr (grouped<DIM, P, VPHASE>()) {
-                if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
-                    if constexpr (VPHASE) v_chunk_g<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
-                    else t_chunk_g<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
-                } else {
-                    if constexpr (VPHASE) v_chunk_g<DIM, ORD, P, false>(S, x0, y, z, r, mask);
-                    else t_chunk_g<DIM, ORD, P, false>(S, x0, y, z, r, mask);
-                }
-            } else if (P::prec == BP_PREC_COMP16 && (r != (R)1 || !BP_RS_SPLIT)) {
-                if constexpr (VPHASE) v_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
-                else t_chunk<DIM, ORD, P, P::prec == BP_PREC_COMP16>(S, x0, y, z, r, mask);
-            } else {
-                if constexpr (VPHASE) v_chunk<DIM, ORD, P, false>(S, x0, y, z, r, mask);
-                else t_chunk<DIM, ORD, P, false>(S, x0, y, z, r, mask);
-            }
-            if constexpr (!VPHASE)
-                if (post) post_chunk<DIM, P>(S, it_cur, x0 + y * (cidx)S.pitch + z * (cidx)S.plane, x0, y, z);
-        };
-        // MU: tiles of more units than warps (16-row or 8 x 2 tiles); the
-        // one-unit form keeps no loop state live across the chunk code, which
-        // costs the 2D FP32 V phase its spill-free 80 registers otherwise
-        if constexpr (MU) {
-            for (int u = warp; u < units; u += kWarps) unit(u);
-        } else {
-            if (warp < units) unit(warp);
-        }
+        tile_units<DIM, ORD, P, VPHASE, MU, true>(S, rb, sb, warp, lane, r, it_cur, post);
     }
 }
 
