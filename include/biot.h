@@ -187,8 +187,12 @@ int bp_set_graph_steps(bp_sim* sim, int steps);
                                rounding, receivers and source inside the stencil
                                border; steps run in pairs, an odd last step of a
                                bp_run by the register kernels */
+#define BP_KERNEL_INTERLEAVED 5 /* one persistent launch per step that interleaves the
+                               V and T phases of the register tiles band by band, so
+                               the T tiles find the V tiles' data in L2 (every dim
+                               and precision; tile shapes of at most 8 units) */
 int bp_set_kernel(bp_sim* sim, int variant);
-/* The family that runs the steps (BP_KERNEL_REGISTER .. BP_KERNEL_FUSED). */
+/* The family that runs the steps (BP_KERNEL_REGISTER .. BP_KERNEL_INTERLEAVED). */
 int bp_get_kernel(bp_sim* sim, int* variant);
 
 /* Step index of the next step to run (it). */
@@ -375,8 +379,9 @@ typedef struct bp_tune {
     int tile_segs;        /* 128-cell x segments per tile, 1..4 (0 = 1)        */
     int tile_tz;          /* 3D: z planes among the tile's rows, 1..tile_rows
                              (0 = the precision's default)                    */
-    int kernel;           /* BP_KERNEL_* family; 0 = autotune (2D FP32/COMP16:
-                             the register tiles or the fused step kernel)     */
+    int kernel;           /* BP_KERNEL_* family; 0 = autotune among the register
+                             tiles, the interleaved kernel and (2D) the fused
+                             step kernel                                      */
     int reserved[2];
 } bp_tune;
 

@@ -22,7 +22,7 @@ TRACES = ["txx", "tzz", "vux", "vwx", "p"]          # sisx sisz sisvu sisvw sisp
 TRACE = {n: i for i, n in enumerate(TRACES)}
 SRC_TAU, SRC_P = 1, 2
 ROUND = {"fast": 0, "reference": 1}
-KERNELS = {"auto": 0, "register": 1, "staged": 2, "march": 3, "fused": 4}
+KERNELS = {"auto": 0, "register": 1, "staged": 2, "march": 3, "fused": 4, "interleaved": 5}
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 COEFS = ["rho_x", "rho_y", "rho_z", "rhof", "cc1_x", "cc1_y", "cc1_z", "cc2_x", "cc2_y", "cc2_z",
          "C", "M", "H", "H2u", "mu_xy", "mu_xz", "mu_yz"]

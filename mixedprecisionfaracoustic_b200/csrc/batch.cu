@@ -47,7 +47,11 @@ int BatchCore::rebuild() {
     std::vector<ShotDesc> h(n);
     long long t0 = 0;
     int maxrec = 0;
-    long long t0s = 0, t0m = 0, t0f = 0;
+    long long t0s = 0, t0m = 0, t0f = 0, t0i = 0;
+    int nbands = 0, dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ctas_i = inter_occupancy(prec, dim, order, rounding) * sms;
     bool all_fused = true;
     const TileShape ts = effective_shape();
     for (int i = 0; i < n; i++) {
@@ -57,6 +61,10 @@ int BatchCore::rebuild() {
         h[i].tile0s = t0s;
         h[i].tile0m = t0m;
         h[i].tile0f = t0f;
+        h[i].item0_i = t0i;
+        h[i].band0_i = nbands;
+        t0i += apply_bands(h[i], dim, tiles, ctas_i);
+        nbands += h[i].nbands_i;
         h[i].done = 0;
         t0f += shots[i]->ntiles_f;
         all_fused = all_fused && shots[i]->ntiles_f > 0;
@@ -74,6 +82,8 @@ int BatchCore::rebuild() {
     for (auto& sh : shots) run.post_in_t = run.post_in_t && sh->post_in_t;
     run.rounding = rounding;
     run.ntiles_f = all_fused ? t0f : 0;
+    run.nitems_i = t0i;
+    run.nbands_i = nbands;
     run.variant = kernel;
     run.multi_unit = ts.rows * ts.segs > phase_threads() / 32;
     run.configure(prec, dim, order, d_descs, n, t0, t0s, t0m, maxrec, st, ctas_per_sm,
@@ -175,18 +185,20 @@ int BatchCore::autotune(int budget_steps) {
     // register tiles at their default shape)
     bool can_fused = fused_supported(prec, dim) && rounding == BP_ROUND_FAST;
     for (auto& s : shots) can_fused = can_fused && s->ntiles_f > 0;
-    if (!fix_k && can_fused) {
+    if (!fix_k) {
         const TuneVal base = bv;
-        for (int kern : {BP_KERNEL_REGISTER, BP_KERNEL_FUSED})
+        for (int kern : {BP_KERNEL_REGISTER, BP_KERNEL_INTERLEAVED, BP_KERNEL_FUSED}) {
+            if (kern == BP_KERNEL_FUSED && !can_fused) continue;
             if (!trial(base.ctas_per_sm, base.steps_per_sync, base.shape, kern, &rc) && rc) break;
+        }
     }
     // stage 1: tile shape of the register kernels (at the current CTA count and 32 steps per sync)
-    if (!rc && !fix_shape && bv.kernel != BP_KERNEL_FUSED)
+    if (!rc && !fix_shape && bv.kernel == BP_KERNEL_REGISTER)
         for (const TileShape& ts : shape_candidates(dim, prec))
             if (!(best < 1e30 && ts.rows == bv.shape.rows && ts.segs == bv.shape.segs && ts.tz == bv.shape.tz))
                 if (!trial(bv.ctas_per_sm, bv.steps_per_sync, ts, bv.kernel, &rc) && rc) break;
     // stage 2: persistent CTAs per SM (register tiles)
-    if (!rc && !fix_c && bv.kernel != BP_KERNEL_FUSED) {
+    if (!rc && !fix_c && bv.kernel == BP_KERNEL_REGISTER) {
         const int occ = std::min(phase_occupancy(prec, dim, order, true, rounding),
                                  phase_occupancy(prec, dim, order, false, rounding));
         std::vector<int> ctas = {0};
@@ -280,7 +292,7 @@ int bp_batch_create(const bp_config* cfgs, const bp_medium* media, int nshots, c
             }
             b->core.shape = t;
         }
-        if (tune->kernel < BP_KERNEL_AUTO || tune->kernel > BP_KERNEL_FUSED ||
+        if (tune->kernel < BP_KERNEL_AUTO || tune->kernel > BP_KERNEL_INTERLEAVED ||
             (tune->kernel == BP_KERNEL_FUSED && !(fused_supported(cfgs[0].precision, cfgs[0].dim) &&
                                                  cfgs[0].rounding == BP_ROUND_FAST))) {
             set_error("bad kernel family for this batch");

@@ -118,6 +118,14 @@ struct ShotDesc {
     void* psiVb[3];
     long long tile0f;             // first task of this shot in the fused tiling
     int ncol_f, zseg_f, nzs_f, pad_f;
+    // the interleaved step kernel (step_inter.cu): the shot's register tiles
+    // grouped into bands of band_t consecutive tiles (whole row blocks; the
+    // last band holds band_last), and its V and T work items in the order
+    // V(0) .. V(lag_i - 1), then T(0), V(lag_i), T(1), V(lag_i + 1), ..., then
+    // the remaining T; item0_i = the shot's first item, band0_i = its first
+    // band counter
+    long long item0_i;
+    int band_t, nbands_i, lag_i, band_last, band0_i, pad_i;
     template <class R>
     __device__ __forceinline__ R dtr() const { return sizeof(R) == 8 ? (R)dtd : (R)dt; }
 };

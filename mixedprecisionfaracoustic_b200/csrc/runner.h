@@ -36,6 +36,12 @@ struct Runner {
     int grid_f = 1;
     bool fused = false;
     long long graph_launches = 0;      // kernels one replay of the captured graph runs
+    long long nitems_i = 0;            // work items of the interleaved step kernel
+    int nbands_i = 0;                  // band counters of all shots
+    int grid_i = 1;
+    bool inter = false;
+    unsigned long long* d_ctl = nullptr;   // its claim counter and band counters (arena cache)
+    size_t d_ctl_bytes = 0, d_ctl_used = 0;
 
     void configure(int prec_, int dim_, int order_, const ShotDesc* d, int n, long long tiles, long long tiles_s,
                    long long tiles_m, int maxrec, cudaStream_t s, int ctas_per_sm, int steps_per_graph) {
@@ -49,29 +55,39 @@ struct Runner {
         long long gv = (long long)ov * sms, gt = (long long)ot * sms;
         grid_v = (int)(gv < tiles ? gv : (tiles > 0 ? tiles : 1));
         grid_t = (int)(gt < tiles ? gt : (tiles > 0 ? tiles : 1));
-        select_kernels();
         grid_s = (int)(sms < tiles_s ? sms : (tiles_s > 0 ? tiles_s : 1));
         if (fused_supported(prec, dim)) grid_f = fused_occupancy(prec, order) * sms;
+        grid_i = inter_occupancy(prec, dim, order, rounding) * sms;
+        d_ctl_used = 8 + 4 * (size_t)(nbands_i > 0 ? nbands_i : 1);
+        if (d_ctl && d_ctl_bytes < d_ctl_used) { arena_release(d_ctl, d_ctl_bytes); d_ctl = nullptr; }
+        if (!d_ctl && nbands_i > 0 &&
+            arena_alloc(d_ctl_used < 256 ? 256 : d_ctl_used, (void**)&d_ctl, &d_ctl_bytes) != cudaSuccess)
+            d_ctl = nullptr;
         if (!d_err) {
             // from the arena cache: a cudaFree, even of 4 bytes, stalled the
             // host for up to 0.6 s when the simulation was destroyed
             if (arena_alloc(256, (void**)&d_err, &d_err_bytes) == cudaSuccess) cudaMemsetAsync(d_err, 0, sizeof(int), st);
             else d_err = nullptr;
         }
+        select_kernels();                  // after the allocations it depends on
         graph_steps = steps_per_graph;
         reset_graph();
     }
     void select_kernels() {
         const bool can_f = fused_supported(prec, dim) && ntiles_f > 0 && rounding == BP_ROUND_FAST;
         fused = can_f && (variant == BP_KERNEL_FUSED || (variant == BP_KERNEL_AUTO && fused_default()));
+        const bool can_i = nitems_i > 0 && d_ctl && d_err && !multi_unit;
+        inter = !fused && can_i && (variant == BP_KERNEL_INTERLEAVED || (variant == BP_KERNEL_AUTO && inter_default()));
         const bool can_m = march_supported(prec, dim) && ntiles_m > 0 && rounding == BP_ROUND_FAST;
-        march = !fused && can_m && (variant == BP_KERNEL_MARCH || (variant == BP_KERNEL_AUTO && march_default()));
+        march = !fused && !inter && can_m &&
+                (variant == BP_KERNEL_MARCH || (variant == BP_KERNEL_AUTO && march_default()));
         const bool can = staged_supported(prec, dim) && ntiles_s > 0 && rounding == BP_ROUND_FAST;
-        staged = !fused && !march && can &&
+        staged = !fused && !inter && !march && can &&
                  (variant == BP_KERNEL_STAGED || (variant == BP_KERNEL_AUTO && staged_default()));
     }
     int family() const {
-        return fused ? BP_KERNEL_FUSED : march ? BP_KERNEL_MARCH : staged ? BP_KERNEL_STAGED : BP_KERNEL_REGISTER;
+        return fused ? BP_KERNEL_FUSED : inter ? BP_KERNEL_INTERLEAVED : march ? BP_KERNEL_MARCH
+               : staged ? BP_KERNEL_STAGED : BP_KERNEL_REGISTER;
     }
     void reset_graph() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -83,6 +99,7 @@ struct Runner {
     ~Runner() {
         reset_graph();
         if (d_err) arena_release(d_err, d_err_bytes);
+        if (d_ctl) arena_release(d_ctl, d_ctl_bytes);
     }
 
     // The register kernels' T phase records the receivers and injects the
@@ -103,8 +120,18 @@ struct Runner {
                             (!v && fused_post()) ? 1 : 0, rounding, multi_unit);
     }
 
-    // One step (index k of the chunk) of the two-phase kernels.
+    // One step (index k of the chunk) of the two-phase kernels, or of the
+    // interleaved kernel (its counters zeroed first).
     cudaError_t tile_step(int k, long long* n) {
+        if (inter) {
+            cudaError_t e = cudaMemsetAsync(d_ctl, 0, d_ctl_used, st);
+            if (e == cudaSuccess)
+                e = launch_inter(prec, dim, order, rounding, d_shots, nshots, nitems_i, k, fused_post() ? 1 : 0,
+                                 grid_i, d_ctl, d_err, st);
+            if (e == cudaSuccess && !fused_post()) e = launch_post(prec, d_shots, nshots, max_rec, k, 1, st);
+            *n += fused_post() ? 1 : 2;
+            return e;
+        }
         cudaError_t e = phase(true, k);
         if (e == cudaSuccess) e = phase(false, k);
         if (e == cudaSuccess && !fused_post()) e = launch_post(prec, d_shots, nshots, max_rec, k, 1, st);

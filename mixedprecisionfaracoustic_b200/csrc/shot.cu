@@ -481,6 +481,14 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     if (e == cudaSuccess && nurec > 0)
         e = cudaMemcpyAsync((void*)S.rec_xu, xu.data(), (size_t)nurec * 8, cudaMemcpyHostToDevice, st);
     ntiles = apply_tile_shape(S, dim, c->precision, default_tile_shape(dim, c->precision));
+    {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        S.item0_i = 0;
+        S.band0_i = 0;
+        nitems_i = apply_bands(S, dim, ntiles, inter_occupancy(c->precision, dim, c->order, c->rounding) * sms);
+    }
     d_desc = (ShotDesc*)(A + p.o_desc);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_desc, &S, sizeof(ShotDesc), cudaMemcpyHostToDevice, st);

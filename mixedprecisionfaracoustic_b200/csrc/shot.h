@@ -39,6 +39,16 @@ TileShape default_tile_shape(int dim, int prec);
 bool valid_tile_shape(int dim, const TileShape& t);
 // Writes the shape into the descriptor and returns the shot's tile count.
 long long apply_tile_shape(ShotDesc& S, int dim, int prec, TileShape t);
+// Groups the shot's tiles (current shape, ntiles of them) into the bands of
+// the interleaved step kernel, for a launch of `ctas` persistent CTAs; returns
+// the shot's work items (2 x ntiles).
+long long apply_bands(ShotDesc& S, int dim, long long ntiles, int ctas);
+bool inter_default();            // whether BP_KERNEL_AUTO picks the interleaved kernel
+int inter_occupancy(int prec, int dim, int order, int rounding);
+// one step of the interleaved kernel; ctl: claim counter (8 bytes) and the
+// bands' completion counters, zeroed before the launch; err: timeout flag
+cudaError_t launch_inter(int prec, int dim, int order, int rounding, const ShotDesc* d, int nshots, long long nitems,
+                         int k, int post, int grid, unsigned long long* ctl, int* err, cudaStream_t st);
 int seg_cells();
 // TMA-staged 2D phase kernels (step_staged.cu)
 bool staged_supported(int prec, int dim);
@@ -110,6 +120,7 @@ struct Shot {
     long long ntiles_s = 0;            // tiles of the TMA-staged 2D kernels (256 x staged_tile_rows)
     long long ntiles_m = 0;            // tasks of the marching 2D kernels (128 cells x zseg_m rows)
     long long ntiles_f = 0;            // tasks of the fused 2D step kernel (120 cells x zseg_f rows), 0 = none
+    long long nitems_i = 0;            // work items of the interleaved step kernel (default tile shape)
     bool post_in_t = false;            // receivers and source all in cells the T phase visits
 
     // The device regions that make up the shot's evolving state, in a fixed

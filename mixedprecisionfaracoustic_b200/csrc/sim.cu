@@ -145,6 +145,8 @@ int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out) {
     s->run.post_in_t = s->shot.post_in_t;
     s->run.rounding = cfg->rounding;
     s->run.ntiles_f = s->shot.ntiles_f;
+    s->run.nitems_i = s->shot.nitems_i;
+    s->run.nbands_i = s->shot.desc.nbands_i;
     s->run.configure(cfg->precision, cfg->dim, cfg->order, s->shot.d_desc, 1, s->shot.ntiles, s->shot.ntiles_s,
                      s->shot.ntiles_m, s->shot.nurec, s->st, 0, 32);
     *out = s;
@@ -202,7 +204,7 @@ int bp_sync(bp_sim* s) {
     if (!s) { set_error("null sim"); return BP_ERR_ARG; }
     SIM_CK(cudaStreamSynchronize(s->st));
     int rc = s->run.device_error();
-    if (rc) { set_error("a staged phase kernel gave up waiting for its tile copies"); return rc; }
+    if (rc) { set_error("a step kernel gave up waiting (staged tile copies or interleaved band counters)"); return rc; }
     const int bad = s->shot.blowup_step(s->st);
     if (bad) {
         set_error("non-finite value recorded at a receiver at step " + std::to_string(bad - 1) +
@@ -221,7 +223,7 @@ int bp_set_graph_steps(bp_sim* s, int steps) {
 }
 
 int bp_set_kernel(bp_sim* s, int variant) {
-    if (!s || variant < BP_KERNEL_AUTO || variant > BP_KERNEL_FUSED) { set_error("bad arguments"); return BP_ERR_ARG; }
+    if (!s || variant < BP_KERNEL_AUTO || variant > BP_KERNEL_INTERLEAVED) { set_error("bad arguments"); return BP_ERR_ARG; }
     if (variant == BP_KERNEL_FUSED && (s->shot.ntiles_f <= 0 || s->shot.cfg.rounding != BP_ROUND_FAST)) {
         set_error("the fused step kernel covers 2D FP32 and COMP16 with fast rounding, receivers and source "
                   "inside the stencil border");
@@ -233,6 +235,10 @@ int bp_set_kernel(bp_sim* s, int variant) {
     }
     if (variant == BP_KERNEL_MARCH && !march_supported(s->shot.cfg.precision, s->shot.cfg.dim)) {
         set_error("the marching kernels cover 2D FP32 and COMP16 only");
+        return BP_ERR_ARG;
+    }
+    if (variant == BP_KERNEL_INTERLEAVED && (s->shot.nitems_i <= 0 || !s->run.d_ctl || !s->run.d_err)) {
+        set_error("the interleaved step kernel has no control block for this simulation");
         return BP_ERR_ARG;
     }
     if ((variant == BP_KERNEL_STAGED || variant == BP_KERNEL_MARCH) && s->shot.cfg.rounding != BP_ROUND_FAST) {
@@ -528,7 +534,7 @@ int bp_algorithmic_bytes(bp_sim* s, double bpc[2], long long* cells) {
 
 int bp_launches_per_step(bp_sim* s, int* n) {
     if (!s || !n) { set_error("bad arguments"); return BP_ERR_ARG; }
-    *n = s->run.fused ? 1 : s->run.launches_per_step();
+    *n = s->run.fused ? 1 : (s->run.inter ? (s->run.fused_post() ? 1 : 2) : s->run.launches_per_step());
     return BP_OK;
 }
 
