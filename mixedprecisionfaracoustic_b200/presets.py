@@ -29,6 +29,7 @@ m = 8 (the reference's porousm, Float/main.cu:1599).
 """
 from __future__ import annotations
 
+import functools
 import math
 
 import numpy as np
@@ -154,6 +155,10 @@ def layered_medium(nx: int, nz: int, seed: int, depth_scale: float = 1.0, host: 
     return med, _vmax(coefs)
 
 
+def _layered_only(nx: int, nz: int, seed: int, depth_scale: float) -> Medium:
+    return layered_medium(nx, nz, seed, depth_scale=depth_scale)[0]
+
+
 def config1(precision: str = "fp32", seed: int = 1, nx: int = 4000, nz: int = 2000, nt: int = 8000,
             npml: int = 20, order: int = 2, nrec: int = 2000, host: bool = False):
     """c1: 2D x-z layered model (scaled by nx, nz for tests).  host=True forms
@@ -266,8 +271,12 @@ def config3_shots(seed: int = 3, nshots: int = 64, nt: int = 4000, precision: st
 
 
 def config4_requests(seed: int = 4, n: int = 1000, precision: str = "fp32", scale: float = 1.0,
-                     steps=(1000, 6000), include_3d: bool = True, npml: int = 20):
-    """c4: request list (cfg, medium) for the serving stream; sizes are scaled by `scale`."""
+                     steps=(1000, 6000), include_3d: bool = True, npml: int = 20, lazy: bool = False):
+    """c4: request list (cfg, medium) for the serving stream; sizes are scaled by `scale`.
+    lazy=True gives, in place of each medium, a function that builds it (the
+    full-size stream's media add up to hundreds of GB on the host; built one
+    at a time at submission, each is freed once the server holds its copy).
+    The configurations and media are the same either way."""
     rng = np.random.default_rng(seed)
     reqs = []
     for i in range(n):
@@ -283,16 +292,19 @@ def config4_requests(seed: int = 4, n: int = 1000, precision: str = "fp32", scal
                              rec_y=None or [], rec_z=[])
             nr = len(cfg.rec_x)
             cfg.rec_y, cfg.rec_z = [ctr] * nr, [npml + 2] * nr
-            reqs.append((cfg, uniform_medium((e, e, e), co)))
+            build = functools.partial(uniform_medium, (e, e, e), co)
+            reqs.append((cfg, build if lazy else build()))
         else:
             nx = max(16, int(rng.integers(512, 2049) * scale))
             nz = max(16, int(rng.integers(512, 2049) * scale))
-            med, vmax = layered_medium(nx, nz, seed=5000 + i, depth_scale=nz / 2000.0)
+            coefs, _ = layered_coefficients(5000 + i)
+            vmax = _vmax(coefs)
+            build = functools.partial(_layered_only, nx, nz, 5000 + i, nz / 2000.0)
             nrec = min(256, nx)
             rx = [npml + (k * nx) // nrec for k in range(nrec)]
             cfg = ShotConfig(dim=2, nx=nx, ny=1, nz=nz, npml=npml, order=2, precision=precision, nt=nt, dx=DX,
                              dt=DT, f0=float(rng.uniform(15, 40)), pml_v0=vmax,
                              src=(npml + nx // 2, 0, npml + 2), src_mask=_abi.SRC_TAU | _abi.SRC_P,
                              rec_x=rx, rec_y=[0] * nrec, rec_z=[npml + 2] * nrec)
-            reqs.append((cfg, med))
+            reqs.append((cfg, build if lazy else build()))
     return reqs
