@@ -181,8 +181,8 @@ int BatchCore::autotune(int budget_steps) {
         return true;
     };
     int rc = BP_OK;
-    // stage 0: kernel family (2D FP32/COMP16: the fused step kernel against the
-    // register tiles at their default shape)
+    // stage 0: kernel family at the default tile shape: register tiles,
+    // interleaved step, and (2D) the fused step kernel
     bool can_fused = fused_supported(prec, dim) && rounding == BP_ROUND_FAST;
     for (auto& s : shots) can_fused = can_fused && s->ntiles_f > 0;
     if (!fix_k) {
@@ -192,8 +192,9 @@ int BatchCore::autotune(int budget_steps) {
             if (!trial(base.ctas_per_sm, base.steps_per_sync, base.shape, kern, &rc) && rc) break;
         }
     }
-    // stage 1: tile shape of the register kernels (at the current CTA count and 32 steps per sync)
-    if (!rc && !fix_shape && bv.kernel == BP_KERNEL_REGISTER)
+    // stage 1: tile shape of the register or interleaved kernels (at the
+    // current CTA count and 32 steps per sync)
+    if (!rc && !fix_shape && (bv.kernel == BP_KERNEL_REGISTER || bv.kernel == BP_KERNEL_INTERLEAVED))
         for (const TileShape& ts : shape_candidates(dim, prec))
             if (!(best < 1e30 && ts.rows == bv.shape.rows && ts.segs == bv.shape.segs && ts.tz == bv.shape.tz))
                 if (!trial(bv.ctas_per_sm, bv.steps_per_sync, ts, bv.kernel, &rc) && rc) break;

@@ -1,6 +1,6 @@
-"""The interleaved step kernel (one persistent launch per step; V and T tiles
-of bands claimed in order, each T tile waiting for the V tiles of its own and
-the neighbouring bands) against the two-phase register kernels: the same
+"""The interleaved step kernel (one persistent launch per step; V and T units
+of bands claimed in order by the warps, each T unit waiting for the V units of
+its own and the neighbouring bands) against the two-phase register kernels: the same
 per-chunk code, so every trace and field must be bit-identical (tolerance 0)
 in 2D and 3D, at every precision and order, with the source and receivers
 recorded by the T tiles or by the post-step kernel, alone and batched."""
@@ -62,8 +62,11 @@ def test_interleaved_reference_rounding_and_post_kernel():
     check(cfg, med, F2, 120)
 
 
-@pytest.mark.parametrize("prec", ["fp32", "comp16"])
-def test_interleaved_batch_equals_single_shots(prec):
+@pytest.mark.parametrize("prec,tile", [("fp32", (8, 1)), ("comp16", (8, 1)), ("fp32", (16, 1)), ("fp32", (8, 2)),
+                                       ("cbf16", (4, 1))])
+def test_interleaved_batch_equals_single_shots(prec, tile):
+    """Batches at several tile shapes, including tiles of more units (a warp's
+    rows of one segment) than a CTA has warps: every unit is an item of its own."""
     shots = config3_shots(seed=15, nshots=5, nt=140, precision=prec, scale=0.1)
     shots[1][0].nt = 71
     singles = []
@@ -71,7 +74,7 @@ def test_interleaved_batch_equals_single_shots(prec):
         with Simulation(c, m) as s:
             s.run(c.nt)
             singles.append((s.traces("txx"), s.traces("p")))
-    b = Batch([c for c, _ in shots], [m for _, m in shots], steps_per_sync=32, ctas_per_sm=0, tile=(8, 1),
+    b = Batch([c for c, _ in shots], [m for _, m in shots], steps_per_sync=32, ctas_per_sm=0, tile=tile,
               kernel="interleaved")
     assert b.tune()["kernel"] == "interleaved"
     b.run(140)
