@@ -306,6 +306,14 @@ int bp_launch_count(bp_sim* sim, long long* n);
  * rounded half away from zero and clamped to +-127; v ~ hi + lo * unit. */
 int bp_comp16_encode(const float* host, size_t n, uint16_t* hi, int8_t* lo);
 int bp_comp16_decode(const uint16_t* hi, const int8_t* lo, size_t n, float* out);
+/* The CBF16 storage codec on the device (BP_PREC_CBF16; no counterpart in the
+ * reference, whose compensated format is COMP16's), over host arrays of n <=
+ * 2^31 values: the top 24 bits of each fp32 word rounded to nearest even at
+ * bit 8 (inf stays inf, a NaN stays a NaN), hi = bits 31..16, lo = bits
+ * 15..8; decode: value bits = hi << 16 | lo << 8.  The kernels' own 4-value
+ * vector forms, the last n mod 4 values through the scalar ones. */
+int bp_cbf16_encode(const float* host, size_t n, uint16_t* hi, uint8_t* lo);
+int bp_cbf16_decode(const uint16_t* hi, const uint8_t* lo, size_t n, float* out);
 
 /* Relative L2 difference ||x - ref|| / ||ref|| of two DEVICE float arrays of
  * n elements, accumulated in FP64 with warp-shuffle reductions.  Allocates

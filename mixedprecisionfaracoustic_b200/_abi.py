@@ -99,6 +99,8 @@ _SIGS = [
     ("bp_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     ("bp_comp16_encode", C.c_int, [FloatP, C.c_size_t, C.POINTER(C.c_uint16), C.POINTER(C.c_int8)]),
     ("bp_comp16_decode", C.c_int, [C.POINTER(C.c_uint16), C.POINTER(C.c_int8), C.c_size_t, FloatP]),
+    ("bp_cbf16_encode", C.c_int, [FloatP, C.c_size_t, C.POINTER(C.c_uint16), C.POINTER(C.c_uint8)]),
+    ("bp_cbf16_decode", C.c_int, [C.POINTER(C.c_uint16), C.POINTER(C.c_uint8), C.c_size_t, FloatP]),
     ("bp_rel_l2_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, DoubleP]),
     ("bp_rel_l2_device_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, DoubleP]),
     ("bp_trace_rel_l2", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, DoubleP]),

@@ -192,9 +192,8 @@ int BatchCore::autotune(int budget_steps) {
             if (!trial(base.ctas_per_sm, base.steps_per_sync, base.shape, kern, &rc) && rc) break;
         }
     }
-    // stage 1: tile shape of the register or interleaved kernels (at the
-    // current CTA count and 32 steps per sync)
-    if (!rc && !fix_shape && (bv.kernel == BP_KERNEL_REGISTER || bv.kernel == BP_KERNEL_INTERLEAVED))
+    // stage 1: tile shape of the register kernels (at the current CTA count and 32 steps per sync)
+    if (!rc && !fix_shape && bv.kernel == BP_KERNEL_REGISTER)
         for (const TileShape& ts : shape_candidates(dim, prec))
             if (!(best < 1e30 && ts.rows == bv.shape.rows && ts.segs == bv.shape.segs && ts.tz == bv.shape.tz))
                 if (!trial(bv.ctas_per_sm, bv.steps_per_sync, ts, bv.kernel, &rc) && rc) break;

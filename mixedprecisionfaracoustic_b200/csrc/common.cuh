@@ -289,48 +289,52 @@ struct PolF32R : PolF32 {
 // fp32 exponent range, so no exponent scaling or rescale; decoding places two
 // bytes.  Arithmetic is FP32's (PolF32's prec), storage 3 bytes per value like
 // COMP16.
-__device__ __forceinline__ unsigned b24_round(float v) {
+// The rounded word in place: bits 31..8 hold the 24-bit value, bits 7..0
+// are don't-care (the stores take bytes 1..3 of it).
+__device__ __forceinline__ unsigned b24_round_word(float v) {
     const unsigned b = __float_as_uint(v);
-    if ((b & 0x7f800000u) == 0x7f800000u) return (b >> 8) | ((b & 0x007fffffu) ? 1u : 0u);   // inf / nan
-    return (b + 0x7fu + ((b >> 8) & 1u)) >> 8;                                                  // RNE at bit 8
+    if ((b & 0x7f800000u) == 0x7f800000u) return b | ((b & 0x007fffffu) ? 0x100u : 0u);   // inf / nan
+    return b + 0x7fu + ((b >> 8) & 1u);                                                  // RNE at bit 8
 }
-__device__ __forceinline__ float b24_value(unsigned w) { return __uint_as_float(w << 8); }
 
 struct PolB24 : PolF32 {
     static constexpr int store = BP_PREC_CBF16;
+    // Decoding and packing are byte moves (__byte_perm): value j of a 4-cell
+    // group is [0, lo_j, hi_j.lo, hi_j.hi] from the low byte up.
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t* lo, cidx i, real (&v)[4]) {
         const uint2 h = ldv<NC>(reinterpret_cast<const uint2*>(static_cast<const uint16_t*>(p) + i));
         const unsigned l = ldv<NC>(reinterpret_cast<const unsigned*>(lo + i));
-        v[0] = __uint_as_float((h.x << 16) | ((l << 8) & 0xff00u));
-        v[1] = __uint_as_float((h.x & 0xffff0000u) | (l & 0xff00u));
-        v[2] = __uint_as_float((h.y << 16) | ((l >> 8) & 0xff00u));
-        v[3] = __uint_as_float((h.y & 0xffff0000u) | ((l >> 16) & 0xff00u));
+        const unsigned y = l << 8, y2 = l >> 8;        // [0, l0, l1, l2], [l1, l2, l3, 0]
+        v[0] = __uint_as_float(__byte_perm(h.x, y, 0x1054));
+        v[1] = __uint_as_float(__byte_perm(h.x, y, 0x3264));
+        v[2] = __uint_as_float(__byte_perm(h.y, y, 0x1074));
+        v[3] = __uint_as_float(__byte_perm(h.y, y2, 0x3267));
     }
     template <bool NC = false>
     __device__ __forceinline__ static real ld1(const void* p, const int8_t* lo, cidx i) {
         const unsigned h = ldv<NC>(static_cast<const uint16_t*>(p) + i);
         const unsigned l = (unsigned char)ldv<NC>(reinterpret_cast<const signed char*>(lo) + i);
-        return __uint_as_float((h << 16) | (l << 8));
+        return __uint_as_float(__byte_perm(h, l, 0x1042));
     }
     __device__ __forceinline__ static void st4(void* p, int8_t* lo, cidx i, const real (&v)[4]) {
         unsigned w[4];
 #pragma unroll
-        for (int j = 0; j < 4; j++) w[j] = b24_round(v[j]);
+        for (int j = 0; j < 4; j++) w[j] = b24_round_word(v[j]);
         *reinterpret_cast<uint2*>(static_cast<uint16_t*>(p) + i) =
-            make_uint2((w[0] >> 8) | ((w[1] >> 8) << 16), (w[2] >> 8) | ((w[3] >> 8) << 16));
+            make_uint2(__byte_perm(w[0], w[1], 0x7632), __byte_perm(w[2], w[3], 0x7632));
         *reinterpret_cast<unsigned*>(lo + i) =
-            (w[0] & 0xffu) | ((w[1] & 0xffu) << 8) | ((w[2] & 0xffu) << 16) | ((w[3] & 0xffu) << 24);
+            __byte_perm(__byte_perm(w[0], w[1], 0x0051), __byte_perm(w[2], w[3], 0x0051), 0x5410);
     }
     __device__ __forceinline__ static void st1(void* p, int8_t* lo, cidx i, real v) {
-        const unsigned w = b24_round(v);
-        static_cast<uint16_t*>(p)[i] = (uint16_t)(w >> 8);
-        lo[i] = (int8_t)(unsigned char)(w & 0xffu);
+        const unsigned w = b24_round_word(v);
+        static_cast<uint16_t*>(p)[i] = (uint16_t)(w >> 16);
+        lo[i] = (int8_t)(unsigned char)((w >> 8) & 0xffu);
     }
     __device__ __forceinline__ static void st4_rt(void* p, int8_t* lo, cidx i, real (&v)[4], bool st) {
         if (st) st4(p, lo, i, v);
 #pragma unroll
-        for (int j = 0; j < 4; j++) v[j] = b24_value(b24_round(v[j]));
+        for (int j = 0; j < 4; j++) v[j] = __uint_as_float(b24_round_word(v[j]) & 0xffffff00u);
     }
     // (the raw-load interface of PolF32 does not apply; the marching and staged
     // kernels, its only users, do not take this storage)

@@ -76,7 +76,7 @@ struct Runner {
     void select_kernels() {
         const bool can_f = fused_supported(prec, dim) && ntiles_f > 0 && rounding == BP_ROUND_FAST;
         fused = can_f && (variant == BP_KERNEL_FUSED || (variant == BP_KERNEL_AUTO && fused_default()));
-        const bool can_i = nitems_i > 0 && d_ctl && d_err;
+        const bool can_i = nitems_i > 0 && d_ctl && d_err && !multi_unit;
         inter = !fused && can_i && (variant == BP_KERNEL_INTERLEAVED || (variant == BP_KERNEL_AUTO && inter_default()));
         const bool can_m = march_supported(prec, dim) && ntiles_m > 0 && rounding == BP_ROUND_FAST;
         march = !fused && !inter && can_m &&

@@ -9,24 +9,21 @@
 // The two-phase kernels stream every field through HBM in the V launch and
 // again in the T launch: 144 B per cell and step at FP32 in 2D, where one pass
 // would need 112.  Here a shot's register tiles are grouped into bands of
-// consecutive row blocks, and the work items (one unit -- one warp's rows --
-// of one tile of one phase) are claimed by the warps of the persistent grid
-// from one counter in the order
+// consecutive row blocks, and the work items (one tile of one phase) are
+// claimed by the persistent CTAs from one counter in the order
 //
 //     V(0) .. V(A-1), T(0), V(A), T(1), V(A+1), ..., T(nb-1-A) .. T(nb-1)
 //
-// with A the lag in bands (sized to the items the warps hold).  A stress unit
-// of band b reads new velocities and old stresses of bands b-1..b+1 and
-// overwrites the stresses of band b, which the velocity units of bands
-// b-1..b+1 read: it waits until those three bands' velocity units are all
-// done, and with A >= 2 they all precede it in the order.  Every warp works
-// through its claims in order (one in work, one claimed ahead), so the
-// earliest unfinished item always belongs to a running warp that is working
-// on it, and its dependencies, all earlier, are done: the waits always end.
-// Velocity units wait for nothing.  The waits still poll a bounded number of
-// times; one that runs out sets the error flag (BP_ERR_TIMEOUT at the next
-// sync) and every later wait gives up at once.  Warps claim, wait and count
-// on their own, with no CTA-wide barrier.
+// with A the lag in bands (sized to the CTAs' in-flight window).  A stress
+// tile of band b reads new velocities and old stresses of bands b-1..b+1 and
+// overwrites the stresses of band b, which the velocity tiles of bands b-1..b+1
+// read: it waits until those three bands' velocity tiles are all done, and
+// with A >= 2 they all precede it in the order, so every wait is on work that
+// running CTAs have already claimed (a CTA claims its next item while it works
+// on the current one, and that next item is never a dependency of the
+// current one).  Velocity tiles wait for nothing.  The waits poll a per-band
+// completion counter with a bounded number of polls; one that runs out sets
+// the error flag (BP_ERR_TIMEOUT at the next sync) and proceeds.
 //
 // The per-cell arithmetic is the tile kernels' own (tile.cuh), so the results
 // are bit-identical to the two-phase kernels.  Loads never take the read-only
@@ -77,35 +74,32 @@ __device__ __forceinline__ int locate_shot_i(const ShotDesc* shots, int nshots, 
 }
 
 struct InterItem {
-    int phase;      // 0: velocity unit, 1: stress unit
-    int band, unit; // band of the shot, unit within the band
+    int phase;      // 0: velocity tile, 1: stress tile
+    int band, tile; // band of the shot, tile within the band
 };
 
 // Item j of a shot (see the header for the order of positions; every
-// position holds the units of band_t tiles but those of the last band, which
-// hold band_last tiles' units).  q: the unit within the band.
-__device__ __forceinline__ InterItem decode_item(const ShotDesc& S, long long j, int lu) {
-    const long long tpb = (long long)S.band_t << lu, ntl = (long long)S.band_last << lu;
-    const int nb = S.nbands_i, A = S.lag_i;
+// position holds band_t tiles but those of the last band, band_last).
+__device__ __forceinline__ InterItem decode_item(const ShotDesc& S, long long j) {
+    const int tpb = S.band_t, nb = S.nbands_i, A = S.lag_i, ntl = S.band_last;
     const int K = nb - A;                              // velocity bands after the first A
     const int pv_last = K == 0 ? nb - 1 : A + 2 * K - 1;   // position of V(nb-1)
     const long long lo = (long long)pv_last * tpb;
-    int p;
-    long long q;
+    int p, tile;
     if (j < lo) {
         p = (int)(j / tpb);
-        q = j - (long long)p * tpb;
+        tile = (int)(j - (long long)p * tpb);
     } else if (j < lo + ntl) {
         p = pv_last;
-        q = j - lo;
+        tile = (int)(j - lo);
     } else {
         const long long jj = j - lo - ntl;
-        const int n = (int)(jj / tpb);
-        p = pv_last + 1 + n;
-        q = jj - (long long)n * tpb;
+        const int q = (int)(jj / tpb);
+        p = pv_last + 1 + q;
+        tile = (int)(jj - (long long)q * tpb);
     }
     InterItem I;
-    I.unit = (int)q;
+    I.tile = tile;
     if (p < A) {
         I.phase = 0;
         I.band = p;
@@ -122,50 +116,48 @@ __device__ __forceinline__ InterItem decode_item(const ShotDesc& S, long long j,
     return I;
 }
 
-// Every warp claims, waits and counts on its own: a CTA-wide barrier per item
-// would hold all eight warps to the slowest one's loads.
 template <int DIM, int ORD, class P>
 __global__ void __launch_bounds__(kThreads, (inter_min_blocks<DIM, ORD, P>())) k_inter(
     const ShotDesc* __restrict__ shots, int nshots, long long nitems, int k, int post, unsigned long long* claim,
     int* done, int* err) {
     using R = typename P::real;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __shared__ ShotDesc sdesc[kWarps];                // one copy per warp
-    ShotDesc& S = sdesc[warp];
+    __shared__ ShotDesc sdesc;
+    __shared__ long long s_item;
     int cur = -1;
     unsigned long long next = 0;
-    if (lane == 0) next = atomicAdd(claim, 1ull);
+    if (threadIdx.x == 0) next = atomicAdd(claim, 1ull);
     for (;;) {
-        unsigned long long mine = 0;
-        if (lane == 0) {
-            mine = next;
-            next = atomicAdd(claim, 1ull);              // the item after this one, claimed ahead
+        __syncthreads();                               // the previous item is finished by every thread
+        if (threadIdx.x == 0) {
+            s_item = (long long)next;
+            next = atomicAdd(claim, 1ull);             // the item after this one, claimed ahead
         }
-        const long long j = (long long)__shfl_sync(0xffffffffu, mine, 0);
+        __syncthreads();
+        const long long j = s_item;
         if (j >= nitems) break;
         const int si = nshots == 1 ? 0 : locate_shot_i(shots, nshots, j);
         if (si != cur) {
-            __syncwarp();
             const long long* src = reinterpret_cast<const long long*>(shots + si);
-            long long* dst = reinterpret_cast<long long*>(&S);
-            for (int w = lane; w < (int)(sizeof(ShotDesc) / 8); w += 32) dst[w] = src[w];
-            __syncwarp();
+            long long* dst = reinterpret_cast<long long*>(&sdesc);
+            for (int w = threadIdx.x; w < (int)(sizeof(ShotDesc) / 8); w += blockDim.x) dst[w] = src[w];
+            __syncthreads();
             cur = si;
         }
+        const ShotDesc& S = sdesc;
         const int it = *S.step_base + k;
         if (S.done || it >= S.nt) continue;
         R r = (R)1;
         if constexpr (P::prec == BP_PREC_COMP16) r = S.rtab[it];
-        const int lu = S.tile_lr + S.tile_ls;           // log2 units per tile
-        const InterItem I = decode_item(S, j - S.item0_i, lu);
+        const InterItem I = decode_item(S, j - S.item0_i);
         if (I.phase == 1) {
-            // the velocity units of bands b-1, b, b+1 must all be done
-            if (lane == 0) {
-                const volatile int* ve = err;
+            // the velocity tiles of bands b-1, b, b+1 must all be done
+            if (threadIdx.x == 0) {
                 for (int bb = I.band - 1; bb <= I.band + 1; bb++) {
                     if (bb < 0 || bb >= S.nbands_i) continue;
-                    const int need = (bb == S.nbands_i - 1 ? S.band_last : S.band_t) << lu;
+                    const int need = bb == S.nbands_i - 1 ? S.band_last : S.band_t;
                     const volatile int* c = done + S.band0_i + bb;
+                    const volatile int* ve = err;
                     long long n = 0;
                     // once any wait has given up, the rest give up at once
                     while (*c < need && *ve == 0) {
@@ -178,18 +170,17 @@ __global__ void __launch_bounds__(kThreads, (inter_min_blocks<DIM, ORD, P>())) k
                 }
                 __threadfence();
             }
-            __syncwarp();
+            __syncthreads();
         }
-        const int lt = I.band * S.band_t + (I.unit >> lu);
-        const int u = I.unit & ((1 << lu) - 1);
+        const int lt = I.band * S.band_t + I.tile;
         const int rb = lt / S.nseg_t, sb = lt - rb * S.nseg_t;
         if (I.phase == 0) {
-            tile_units<DIM, ORD, P, true, false, false>(S, rb, sb, u, lane, r, it, 0);
-            __threadfence();                           // the unit's stores before its count
-            __syncwarp();
-            if (lane == 0) atomicAdd(done + S.band0_i + I.band, 1);
+            tile_units<DIM, ORD, P, true, false, false>(S, rb, sb, warp, lane, r, it, 0);
+            __threadfence();                           // this thread's stores before the count
+            __syncthreads();
+            if (threadIdx.x == 0) atomicAdd(done + S.band0_i + I.band, 1);
         } else {
-            tile_units<DIM, ORD, P, false, false, false>(S, rb, sb, u, lane, r, it, post);
+            tile_units<DIM, ORD, P, false, false, false>(S, rb, sb, warp, lane, r, it, post);
         }
     }
 }
@@ -211,17 +202,15 @@ long long apply_bands(ShotDesc& S, int dim, long long ntiles, int ctas) {
     }
     const long long tpb = (long long)rb_per_band * S.nseg_t;
     const int nb = (int)((ntiles + tpb - 1) / tpb);
-    const long long units = 1LL << (S.tile_lr + S.tile_ls);
     S.band_t = (int)tpb;
     S.nbands_i = nb;
     S.band_last = (int)(ntiles - (long long)(nb - 1) * tpb);
     // leading velocity bands: at least 2 (so every wait is on earlier items)
-    // and enough that the items the warps hold (one in work, one claimed
-    // ahead) lie behind the bands a stress unit waits for
-    const long long inflight = 2LL * ctas * kWarps, per_band = tpb * units;
-    const long long want = (inflight + per_band - 1) / per_band + 2;
+    // and enough that the CTAs' in-flight items lie behind the bands a stress
+    // tile waits for
+    const long long want = (ctas + tpb - 1) / tpb + 2;
     S.lag_i = (int)(nb < want ? nb : want);
-    return 2 * ntiles * units;
+    return 2 * ntiles;
 }
 
 template <int DIM, int ORD, class P>
