@@ -239,12 +239,26 @@ def run_ours(args, rank, ws):
                                             {"v_phase": bv, "t_phase": bt}),
                          "step_frac": (bv + bt) * cells / ((pv + pt) * 1e-3) / 1e9 / peak},
             "cells": cells,
+            "medium": (f"indexed: {s.medium_tuples()} coefficient tuples, one index byte per cell"
+                       if s.medium_tuples() else "per-cell coefficient arrays"),
         }
         sims[prec] = s
     if args.only:
         for s in sims.values():
             s.close()
         return res, None
+    # the same FP32 shot reading its per-cell coefficient arrays (what the
+    # indexed medium saves)
+    cfg, med = workload("fp32", max(C1_STEPS, W + K + 64), args.nx, args.nz)
+    cfg.device = dev
+    cfg.medium = "dense"
+    with Simulation(cfg, med) as sd:
+        sd.run_timed(W)
+        ms_d = sd.run_timed(K)
+        (dv, dt_), _ = sd.algorithmic_bytes()
+    res["fp32"]["dense_medium"] = {"value": res["fp32"]["cells"] * K / (ms_d * 1e-3) / 1e6, "unit": METRIC,
+                                   "ms_per_step": ms_d / K, "bytes_per_cell": {"v_phase": dv, "t_phase": dt_},
+                                   "timed_steps": K}
     # FP64 run of the same steps: seismogram relative L2 of both paths
     steps_run = W + 128 + reps * K + P
     cfg, med = workload("fp64", max(C1_STEPS, W + 128 + 4 * K + P), args.nx, args.nz)
@@ -313,10 +327,15 @@ def run_batched(args):
         b = Batch([c for c, _ in shots], [m for _, m in shots])
         tune = b.autotune(tune_budget)
         # algorithmic bytes per updated cell of the step the chosen kernels run:
-        # two phases (each array once per phase) or the fused step (fields once
-        # each way, coefficients once); 4 bytes per value at FP32, 3 otherwise
+        # two phases (each array once per phase: the library's count, an
+        # indexed medium's coefficients as one index byte per phase) or the
+        # fused step (fields once each way, coefficients once)
+        indexed = all(b.medium_tuples(i) > 0 for i in range(len(shots)))
         wb = 4.0 if prec == "fp32" else 3.0
-        bpc = (2 * 8 + 12) * wb if tune["kernel"] == "fused" else (24 + 12) * wb
+        if tune["kernel"] == "fused":
+            bpc = 2 * 8 * wb + (1.0 if indexed else 12 * wb)
+        else:
+            bpc = b.algorithmic_bytes() / cells
         b.run(max(args.warmup, 3))
         b.sync()
         with ClockSampler(0) as clk:
@@ -325,6 +344,8 @@ def run_batched(args):
         got = bpc * cells * K / (ms * 1e-3) / 1e9
         out[prec] = {"value": cells * K / (ms * 1e-3) / 1e6, "unit": METRIC, "ms_per_step": ms / K,
                      "tune": tune, "clocks": clk.summary(),
+                     "medium": ("indexed: " + ", ".join(str(b.medium_tuples(i)) for i in range(3)) + ", ... tuples"
+                                if indexed else "per-cell coefficient arrays"),
                      "roofline": {"bound": "hbm", "kernel": "step", "bytes_per_cell": bpc, "achieved": got,
                                   "peak": peak, "unit": "GB/s", "frac": got / peak, "peak_source": peak_kind}}
         b.close()
@@ -676,14 +697,15 @@ def main():
         batched = None if (args.no_batched or ws > 1) else run_batched(args)
         cpu = None if (args.no_cpu_baseline or ws > 1) else cpu_baseline(args)
         traffic = ncu_traffic()
+        def tkey(prec, r):                 # ncu captures of the same medium representation
+            return f"{prec}_{r['roofline']['kernel']}" + ("_indexed" if r["medium"].startswith("indexed") else "")
         roof = dict(f32["roofline"])
-        tk = traffic.get(f"fp32_{roof['kernel']}")
-        roof["traffic"] = tk
+        roof["traffic"] = traffic.get(tkey("fp32", f32))
         c16roof = dict(c16["roofline"])
-        c16roof["traffic"] = traffic.get(f"comp16_{c16roof['kernel']}")
+        c16roof["traffic"] = traffic.get(tkey("comp16", c16))
         b24 = res["cbf16"]
         b24roof = dict(b24["roofline"])
-        b24roof["traffic"] = traffic.get(f"cbf16_{b24roof['kernel']}")
+        b24roof["traffic"] = traffic.get(tkey("cbf16", b24))
         out = {
             "metric": METRIC, "value": f32["value"], "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": f32["ms_per_step"], "higher_is_better": True,
@@ -697,12 +719,16 @@ def main():
             "rel_l2_vs_fp64": f32["rel_l2_vs_fp64"],
             "timed_regions": f32["timed_regions"],
             "phase_ms": f32["phase_ms"],
+            "medium": f32["medium"],
+            "dense_medium": f32["dense_medium"],
             "comp16": {"value": c16["value"], "ms_per_step": c16["ms_per_step"], "roofline": c16roof,
+                       "medium": c16["medium"],
                        "rel_l2_vs_fp64": c16["rel_l2_vs_fp64"], "phase_ms": c16["phase_ms"],
                        "gpu_launches": c16["launches"], "clocks": c16["clocks"],
                        "timed_regions": c16["timed_regions"],
                        "speedup_vs_fp32": c16["value"] / f32["value"]},
             "cbf16": {"value": b24["value"], "ms_per_step": b24["ms_per_step"], "roofline": b24roof,
+                      "medium": b24["medium"],
                       "storage": "bf16 hi + 8-bit residual (top 24 bits of fp32), fp32 math",
                       "rel_l2_vs_fp64": b24["rel_l2_vs_fp64"], "phase_ms": b24["phase_ms"],
                       "gpu_launches": b24["launches"], "clocks": b24["clocks"],

@@ -50,6 +50,19 @@ extern "C" {
                                to nearest even), fp32 arithmetic as BP_PREC_FP32; no
                                exponent scaling or rescale (bf16 has fp32's range) */
 
+/* How the kernels read the medium (bp_config.medium).  AUTO: when the shot's
+ * cells hold at most 256 distinct coefficient tuples (layered, blocky and
+ * uniform media), each cell keeps a one-byte index into a table of the
+ * decoded tuples, read through L1, in place of its 12 (2D) or 17 (3D)
+ * per-cell coefficient arrays; the values, and so the results, are
+ * bit-identical, and the coefficient traffic falls from 48 B (FP32) or 36 B
+ * (COMP16, CBF16) per cell and step to 2 B.  Shots with more tuples, and FP64
+ * shots, read the arrays.  DENSE: always the arrays.  No reference
+ * counterpart: the reference reads per-cell arrays (Float/main.cu:106-113,
+ * 232-250). */
+#define BP_MEDIUM_AUTO 0
+#define BP_MEDIUM_DENSE 1
+
 /* FP32 rounding (bp_config.rounding).  FAST divides by H with a reciprocal and
  * one residual step (within one ulp of the IEEE quotient) and forms the CPML
  * memory update in float.  REFERENCE rounds both like the reference's Float
@@ -119,7 +132,8 @@ typedef struct bp_config {
     int dyn_scale;        /* COMP16: 1 = ramp the state scale 1 -> 16 (Half/main.cu:116-122) */
     int check_cfl;        /* 1 = refuse dt above the stability limit (BP_ERR_CFL) */
     int rounding;         /* FP32: BP_ROUND_FAST (0) or BP_ROUND_REFERENCE (1)   */
-    int reserved[3];
+    int medium;           /* BP_MEDIUM_AUTO (0) or BP_MEDIUM_DENSE (1), below    */
+    int reserved[2];
 } bp_config;
 
 /* Cell-centred Biot coefficients over the PHYSICAL grid (nz*ny*nx floats each,
@@ -290,8 +304,12 @@ int bp_profile_phases(bp_sim* sim, int nsteps, float ms[3]);
 int bp_profile_fused(bp_sim* sim, int nsteps, float* ms, double* bytes_per_cell);
 
 /* Algorithmic HBM bytes per updated cell of each phase (the roofline
- * numerator) and the number of updated cells per step. */
+ * numerator) and the number of updated cells per step.  An indexed medium
+ * (BP_MEDIUM_AUTO) counts one index byte per phase for its coefficients. */
 int bp_algorithmic_bytes(bp_sim* sim, double bytes_per_cell[2], long long* cells);
+/* Distinct coefficient tuples of an indexed medium, 0 where the shot reads
+ * the per-cell coefficient arrays (BP_MEDIUM_DENSE, FP64, > 256 tuples). */
+int bp_get_medium_tuples(bp_sim* sim, int* ntuples);
 
 /* Kernel launches one step issues (for launch counting): 3 (V phase, T phase,
  * record/inject), or 2 where the T phase records and injects itself. */
@@ -416,6 +434,11 @@ int bp_batch_get_tune(bp_batch* b, bp_tune* chosen);
 int bp_batch_autotune(bp_batch* b, int budget_steps);
 /* Total cell-updates performed so far (all shots). */
 int bp_batch_cell_updates(bp_batch* b, long long* updates);
+/* Shot `shot`'s indexed-medium tuples (0: per-cell arrays), and the
+ * algorithmic HBM bytes of one step of the whole batch (bp_algorithmic_bytes
+ * summed over its shots' updated cells). */
+int bp_batch_medium_tuples(bp_batch* b, int shot, int* ntuples);
+int bp_batch_algorithmic_bytes(bp_batch* b, double* bytes_per_step);
 void bp_batch_destroy(bp_batch* b);
 
 /* ---- serving: admission by HBM budget + continuous batching ------------ */

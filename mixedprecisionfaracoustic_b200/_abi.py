@@ -22,6 +22,7 @@ TRACES = ["txx", "tzz", "vux", "vwx", "p"]          # sisx sisz sisvu sisvw sisp
 TRACE = {n: i for i, n in enumerate(TRACES)}
 SRC_TAU, SRC_P = 1, 2
 ROUND = {"fast": 0, "reference": 1}
+MEDIUM = {"auto": 0, "dense": 1}
 KERNELS = {"auto": 0, "register": 1, "staged": 2, "march": 3, "fused": 4, "interleaved": 5}
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 COEFS = ["rho_x", "rho_y", "rho_z", "rhof", "cc1_x", "cc1_y", "cc1_z", "cc2_x", "cc2_y", "cc2_z",
@@ -44,7 +45,7 @@ class BpConfig(C.Structure):
         ("nrec", C.c_int), ("rec_x", IntP), ("rec_y", IntP), ("rec_z", IntP),
         ("nsnap", C.c_int), ("snap_steps", IntP), ("snap_fields", C.c_uint), ("snap_masks", UIntP),
         ("snap_y", C.c_int), ("device", C.c_int), ("comp_coef_lo", C.c_int), ("dyn_scale", C.c_int),
-        ("check_cfl", C.c_int), ("rounding", C.c_int), ("reserved", C.c_int * 3),
+        ("check_cfl", C.c_int), ("rounding", C.c_int), ("medium", C.c_int), ("reserved", C.c_int * 2),
     ]
 
 
@@ -96,6 +97,7 @@ _SIGS = [
     ("bp_profile_phases", C.c_int, [C.c_void_p, C.c_int, FloatP]),
     ("bp_algorithmic_bytes", C.c_int, [C.c_void_p, DoubleP, C.POINTER(C.c_longlong)]),
     ("bp_launches_per_step", C.c_int, [C.c_void_p, IntP]),
+    ("bp_get_medium_tuples", C.c_int, [C.c_void_p, IntP]),
     ("bp_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     ("bp_comp16_encode", C.c_int, [FloatP, C.c_size_t, C.POINTER(C.c_uint16), C.POINTER(C.c_int8)]),
     ("bp_comp16_decode", C.c_int, [C.POINTER(C.c_uint16), C.POINTER(C.c_int8), C.c_size_t, FloatP]),
@@ -121,6 +123,8 @@ _SIGS = [
     ("bp_batch_get_tune", C.c_int, [C.c_void_p, C.POINTER(BpTune)]),
     ("bp_batch_autotune", C.c_int, [C.c_void_p, C.c_int]),
     ("bp_batch_cell_updates", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    ("bp_batch_medium_tuples", C.c_int, [C.c_void_p, C.c_int, IntP]),
+    ("bp_batch_algorithmic_bytes", C.c_int, [C.c_void_p, DoubleP]),
     ("bp_batch_destroy", None, [C.c_void_p]),
     ("bp_shot_bytes", C.c_int, [C.POINTER(BpConfig), C.POINTER(C.c_size_t)]),
     ("bp_server_create", C.c_int, [C.c_int, C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]),

@@ -53,6 +53,7 @@ class ShotConfig:
     dyn_scale: int = 1
     check_cfl: int = 0
     rounding: str = "fast"                # FP32: "fast" or "reference" (bp_config.rounding)
+    medium: str = "auto"                  # "auto" (indexed where <= 256 tuples) or "dense" (bp_config.medium)
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -89,6 +90,7 @@ class ShotConfig:
         c.snap_y = self.snap_y
         c.device, c.comp_coef_lo, c.dyn_scale, c.check_cfl = self.device, self.comp_coef_lo, self.dyn_scale, self.check_cfl
         c.rounding = _abi.ROUND[self.rounding]
+        c.medium = _abi.MEDIUM[self.medium]
         return c
 
 
@@ -286,6 +288,12 @@ class Simulation:
         check(self.lib.bp_algorithmic_bytes(self.h, b, C.byref(cells)), "bp_algorithmic_bytes")
         return (b[0], b[1]), cells.value
 
+    def medium_tuples(self) -> int:
+        """Distinct coefficient tuples of the indexed medium (0: per-cell arrays)."""
+        n = C.c_int()
+        check(self.lib.bp_get_medium_tuples(self.h, C.byref(n)), "bp_get_medium_tuples")
+        return n.value
+
     def launches_per_step(self) -> int:
         """Kernels one step launches: 3, or 2 where the T phase records the
         receivers and injects the source itself."""
@@ -395,6 +403,17 @@ class Batch:
         n = C.c_longlong()
         check(self.lib.bp_batch_cell_updates(self.h, C.byref(n)), "bp_batch_cell_updates")
         return n.value
+
+    def medium_tuples(self, shot: int) -> int:
+        n = C.c_int()
+        check(self.lib.bp_batch_medium_tuples(self.h, int(shot), C.byref(n)), "bp_batch_medium_tuples")
+        return n.value
+
+    def algorithmic_bytes(self) -> float:
+        """Algorithmic HBM bytes of one step of the whole batch."""
+        v = C.c_double()
+        check(self.lib.bp_batch_algorithmic_bytes(self.h, C.byref(v)), "bp_batch_algorithmic_bytes")
+        return v.value
 
     def close(self):
         if getattr(self, "h", None):

@@ -26,7 +26,7 @@ LIB = PKG / "lib" / "libbiot_b200.so"
 BIN = PKG / "bin" / "biot_reference_run"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-LIB_SOURCES = ["step.cu", "step_inter.cu", "step_fused.cu", "step_staged.cu", "step_march.cu", "precompute.cu", "reduce.cu", "codec.cu", "shot.cu", "sim.cu", "batch.cu", "server.cu", "noalloc.cu",
+LIB_SOURCES = ["step.cu", "step_inter.cu", "step_fused.cu", "step_staged.cu", "step_march.cu", "precompute.cu", "medium_index.cu", "reduce.cu", "codec.cu", "shot.cu", "sim.cu", "batch.cu", "server.cu", "noalloc.cu",
                "medium.cpp"]
 DRIVER = "driver_main.cpp"
 

@@ -86,6 +86,8 @@ int BatchCore::rebuild() {
     run.nbands_i = nbands;
     run.variant = kernel;
     run.multi_unit = ts.rows * ts.segs > phase_threads() / 32;
+    run.indexed = false;
+    for (int i = 0; i < n; i++) run.indexed = run.indexed || shots[i]->med_tuples > 0;
     run.configure(prec, dim, order, d_descs, n, t0, t0s, t0m, maxrec, st, ctas_per_sm,
                   steps_per_sync > 0 ? steps_per_sync : 32);
     return BP_OK;
@@ -416,6 +418,24 @@ int bp_batch_autotune(bp_batch* b, int budget_steps) {
     int rc = b->core.autotune(budget_steps);
     if (rc) return rc;
     b->core.tuned = true;
+    return BP_OK;
+}
+
+int bp_batch_medium_tuples(bp_batch* b, int shot, int* ntuples) {
+    if (!b || !ntuples || shot < 0 || shot >= (int)b->core.shots.size()) { set_error("bad arguments"); return BP_ERR_ARG; }
+    *ntuples = b->core.shots[shot]->med_tuples;
+    return BP_OK;
+}
+
+int bp_batch_algorithmic_bytes(bp_batch* b, double* bytes_per_step) {
+    if (!b || !bytes_per_step) { set_error("bad arguments"); return BP_ERR_ARG; }
+    double sum = 0;
+    for (auto& sh : b->core.shots) {
+        double bpc[2];
+        algorithmic_bpc(sh->cfg, sh->med_tuples > 0, bpc);
+        sum += (bpc[0] + bpc[1]) * (double)sh->cells;
+    }
+    *bytes_per_step = sum;
     return BP_OK;
 }
 

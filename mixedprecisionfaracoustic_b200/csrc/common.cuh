@@ -126,9 +126,31 @@ struct ShotDesc {
     // band counter
     long long item0_i;
     int band_t, nbands_i, lag_i, band_last, band0_i, pad_i;
+    // indexed medium (FP32, COMP16, CBF16): when a shot's cells hold at most
+    // 256 distinct coefficient tuples, med_idx gives each cell the index of its
+    // tuple (one byte, at the cell's offset) and ctab holds the tuples decoded,
+    // kMedRow float4 groups each (MedGroup); null: the per-cell arrays above
+    const uint8_t* med_idx;
+    const float4* ctab;
+    int med_tuples, pad_med;
     template <class R>
     __device__ __forceinline__ R dtr() const { return sizeof(R) == 8 ? (R)dtd : (R)dt; }
 };
+
+// Groups of one indexed-medium tuple, as float4 (x, y, z, w):
+//   V_X = (rho_x, cc1_x, cc2_x, rhof), V_Y / V_Z = (rho, cc1, cc2, 0) of that
+//   axis, T_A = (C, M, H, H2mu), T_B = (mu_xz, mu_xy, mu_yz, 0).
+enum MedGroup { MED_V_X, MED_V_Y, MED_V_Z, MED_T_A, MED_T_B, kMedRow };
+constexpr int kMedMaxTuples = 256;
+
+// The four indices of the chunk at cell offset c (a multiple of 4).
+__device__ __forceinline__ unsigned med_ids(const ShotDesc& S, cidx c) {
+    return __ldg(reinterpret_cast<const unsigned*>(S.med_idx + c));
+}
+// Group g of the tuple of the chunk's cell j.
+__device__ __forceinline__ float4 med_group(const ShotDesc& S, unsigned ids, int j, int g) {
+    return __ldg(S.ctab + ((ids >> (8 * j)) & 0xffu) * kMedRow + g);
+}
 
 // Steps are issued in chunks; step k of a chunk of shot s has index
 // it = *step_base + k.  Reading the base from device memory lets one captured

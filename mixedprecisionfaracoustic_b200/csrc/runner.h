@@ -32,6 +32,7 @@ struct Runner {
     bool post_in_t = false;            // every shot's receivers and source lie in cells the T phase visits
     int rounding = BP_ROUND_FAST;      // FP32 BP_ROUND_REFERENCE: PolF32R register kernels only
     bool multi_unit = false;           // the shots' tile shape has more units than a CTA has warps
+    bool indexed = false;              // some shot reads an indexed medium (not the marching or staged kernels)
     long long ntiles_f = 0;            // tasks of the fused step kernel (0: some shot cannot take it)
     int grid_f = 1;
     bool fused = false;
@@ -78,10 +79,10 @@ struct Runner {
         fused = can_f && (variant == BP_KERNEL_FUSED || (variant == BP_KERNEL_AUTO && fused_default()));
         const bool can_i = nitems_i > 0 && d_ctl && d_err && !multi_unit;
         inter = !fused && can_i && (variant == BP_KERNEL_INTERLEAVED || (variant == BP_KERNEL_AUTO && inter_default()));
-        const bool can_m = march_supported(prec, dim) && ntiles_m > 0 && rounding == BP_ROUND_FAST;
+        const bool can_m = march_supported(prec, dim) && ntiles_m > 0 && rounding == BP_ROUND_FAST && !indexed;
         march = !fused && !inter && can_m &&
                 (variant == BP_KERNEL_MARCH || (variant == BP_KERNEL_AUTO && march_default()));
-        const bool can = staged_supported(prec, dim) && ntiles_s > 0 && rounding == BP_ROUND_FAST;
+        const bool can = staged_supported(prec, dim) && ntiles_s > 0 && rounding == BP_ROUND_FAST && !indexed;
         staged = !fused && !inter && !march && can &&
                  (variant == BP_KERNEL_STAGED || (variant == BP_KERNEL_AUTO && staged_default()));
     }

@@ -46,6 +46,7 @@ int validate_config(const bp_config* c) {
     if (c->order != 2 && c->order != 4) { set_error("order must be 2 or 4"); return BP_ERR_ARG; }
     if (c->precision < BP_PREC_FP32 || c->precision > BP_PREC_CBF16) { set_error("bad precision"); return BP_ERR_ARG; }
     if (c->rounding != BP_ROUND_FAST && c->rounding != BP_ROUND_REFERENCE) { set_error("bad rounding"); return BP_ERR_ARG; }
+    if (c->medium != BP_MEDIUM_AUTO && c->medium != BP_MEDIUM_DENSE) { set_error("bad medium mode"); return BP_ERR_ARG; }
     if (c->rounding == BP_ROUND_REFERENCE && c->precision != BP_PREC_FP32) {
         set_error("reference rounding applies to FP32 only");
         return BP_ERR_ARG;
@@ -110,6 +111,7 @@ struct Plan {
     size_t o_fb[BP_NFIELDS], o_flob[BP_NFIELDS], o_psiVb[3];   // second copy (fused step kernel)
     bool fused;
     size_t o_tr, o_tr64, o_wav, o_dyn, o_rtab, o_rec, o_recrow, o_recxu, o_step, o_blowup, o_snap, o_scratch, o_out, o_desc;
+    size_t o_midx, o_mtab, o_mtmp;            // indexed medium: cell indices, tuple table, build scratch
     size_t total;
     size_t staging;               // transient medium upload
 };
@@ -214,6 +216,12 @@ void make_plan(const bp_config* c, int nurec, Plan& p) {
     p.o_scratch = A.take((size_t)2 * nb * 8);
     p.o_out = A.take(4 * 8);
     p.o_desc = A.take(sizeof(ShotDesc));
+    p.o_midx = p.o_mtab = p.o_mtmp = (size_t)-1;
+    if (prec != BP_PREC_FP64 && c->medium == BP_MEDIUM_AUTO) {
+        p.o_midx = A.take((size_t)p.ncell);
+        p.o_mtab = A.take((size_t)kMedMaxTuples * kMedRow * sizeof(float4));
+        p.o_mtmp = A.take(medium_scratch_bytes());
+    }
     p.total = A.off;
     p.staging = (size_t)9 * c->nx * (dim == 3 ? c->ny : 1) * c->nz * 4;
 }
@@ -401,6 +409,24 @@ int Shot::create(const bp_config* c, const bp_medium* med, cudaStream_t st) {
     {
         cudaError_t e = launch_coefs(c->precision, S, dm, c->nx, dim == 3 ? c->ny : 1, c->nz, c->npml, (double)c->dt, em, st);
         if (e != cudaSuccess) { set_error(std::string("coefficient kernel: ") + cudaGetErrorString(e)); return fail(BP_ERR_CUDA); }
+    }
+    // ---- indexed medium (at most 256 distinct coefficient tuples) ----
+    S.med_idx = nullptr;
+    S.ctab = nullptr;
+    S.med_tuples = 0;
+    med_tuples = 0;
+    if (p.o_midx != (size_t)-1) {
+        uint8_t* midx = (uint8_t*)at(p.o_midx);
+        float4* mtab = (float4*)at(p.o_mtab);
+        int n = 0;
+        cudaError_t e = build_medium_index(c->precision, S, midx, mtab, at(p.o_mtmp), (size_t)p.ncell, &n, st);
+        if (e != cudaSuccess) { set_error(std::string("medium index: ") + cudaGetErrorString(e)); return fail(BP_ERR_CUDA); }
+        if (n > 0) {
+            S.med_idx = midx;
+            S.ctab = mtab;
+            S.med_tuples = n;
+            med_tuples = n;
+        }
     }
     // ---- wavelet, dynamic scale, receivers ----
     std::vector<float> wf(c->nt);

@@ -43,6 +43,11 @@ long long apply_tile_shape(ShotDesc& S, int dim, int prec, TileShape t);
 // the interleaved step kernel, for a launch of `ctas` persistent CTAs; returns
 // the shot's work items (2 x ntiles).
 long long apply_bands(ShotDesc& S, int dim, long long ntiles, int ctas);
+// indexed medium (medium_index.cu): *ntuples = 0 leaves the shot on its arrays
+size_t medium_scratch_bytes();
+void algorithmic_bpc(const bp_config& c, bool indexed, double bpc[2]);   // sim.cu
+cudaError_t build_medium_index(int prec, ShotDesc& S, uint8_t* d_idx, float4* d_tab, void* d_scratch, size_t ncell,
+                               int* ntuples, cudaStream_t st);
 bool inter_default();            // whether BP_KERNEL_AUTO picks the interleaved kernel
 int inter_occupancy(int prec, int dim, int order, int rounding);
 // one step of the interleaved kernel; ctl: claim counter (8 bytes) and the
@@ -121,6 +126,7 @@ struct Shot {
     long long ntiles_m = 0;            // tasks of the marching 2D kernels (128 cells x zseg_m rows)
     long long ntiles_f = 0;            // tasks of the fused 2D step kernel (120 cells x zseg_f rows), 0 = none
     long long nitems_i = 0;            // work items of the interleaved step kernel (default tile shape)
+    int med_tuples = 0;                // indexed medium: distinct coefficient tuples (0 = per-cell arrays)
     bool post_in_t = false;            // receivers and source all in cells the T phase visits
 
     // The device regions that make up the shot's evolving state, in a fixed

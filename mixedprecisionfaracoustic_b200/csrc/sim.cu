@@ -146,6 +146,7 @@ int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out) {
     s->run.rounding = cfg->rounding;
     s->run.ntiles_f = s->shot.ntiles_f;
     s->run.nitems_i = s->shot.nitems_i;
+    s->run.indexed = s->shot.med_tuples > 0;
     s->run.nbands_i = s->shot.desc.nbands_i;
     s->run.configure(cfg->precision, cfg->dim, cfg->order, s->shot.d_desc, 1, s->shot.ntiles, s->shot.ntiles_s,
                      s->shot.ntiles_m, s->shot.nurec, s->st, 0, 32);
@@ -239,6 +240,11 @@ int bp_set_kernel(bp_sim* s, int variant) {
     }
     if (variant == BP_KERNEL_INTERLEAVED && (s->shot.nitems_i <= 0 || !s->run.d_ctl || !s->run.d_err)) {
         set_error("the interleaved step kernel has no control block for this simulation");
+        return BP_ERR_ARG;
+    }
+    if ((variant == BP_KERNEL_STAGED || variant == BP_KERNEL_MARCH) && s->shot.med_tuples > 0) {
+        set_error("the staged and marching kernels read the per-cell coefficient arrays: create the shot with "
+                  "medium = BP_MEDIUM_DENSE");
         return BP_ERR_ARG;
     }
     if ((variant == BP_KERNEL_STAGED || variant == BP_KERNEL_MARCH) && s->shot.cfg.rounding != BP_ROUND_FAST) {
@@ -509,26 +515,46 @@ int bp_profile_phases(bp_sim* s, int nsteps, float ms[3]) {
     return BP_OK;
 }
 
-int bp_algorithmic_bytes(bp_sim* s, double bpc[2], long long* cells) {
-    if (!s || !bpc) { set_error("bad arguments"); return BP_ERR_ARG; }
-    const bp_config& c = s->shot.cfg;
-    // words touched once per phase per updated cell (each array element once;
-    // neighbour re-reads and the slab-only CPML variables not counted):
-    //   V: read stresses+p, read+write vu,vw, read coefficients
-    //   T: read vu,vw, read+write stresses+p, read coefficients
+}  // extern "C"
+
+namespace bpk {
+// Algorithmic HBM bytes per updated cell of each phase: words touched once per
+// phase per updated cell (each array element once; neighbour re-reads and the
+// slab-only CPML variables not counted):
+//   V: read stresses+p, read+write vu,vw, read coefficients
+//   T: read vu,vw, read+write stresses+p, read coefficients
+// An indexed medium reads one index byte per cell and phase in place of the
+// coefficients (its table stays in L1).
+void algorithmic_bpc(const bp_config& c, bool indexed, double bpc[2]) {
     double fb, cb;
     if (c.precision == BP_PREC_FP64) { fb = 8; cb = 8; }
     else if (c.precision == BP_PREC_FP32) { fb = 4; cb = 4; }
     else if (c.precision == BP_PREC_CBF16) { fb = 3; cb = 3; }
     else { fb = 3; cb = c.comp_coef_lo ? 3 : 2; }
+    const int nvc = c.dim == 3 ? 10 : 7, ntc = c.dim == 3 ? 7 : 5;
+    const double v_coef = indexed ? 1.0 : nvc * cb, t_coef = indexed ? 1.0 : ntc * cb;
     if (c.dim == 3) {
-        bpc[0] = (7 + 2 * 6) * fb + 10 * cb;
-        bpc[1] = (6 + 2 * 7) * fb + 7 * cb;
+        bpc[0] = (7 + 2 * 6) * fb + v_coef;
+        bpc[1] = (6 + 2 * 7) * fb + t_coef;
     } else {
-        bpc[0] = (4 + 2 * 4) * fb + 7 * cb;
-        bpc[1] = (4 + 2 * 4) * fb + 5 * cb;
+        bpc[0] = (4 + 2 * 4) * fb + v_coef;
+        bpc[1] = (4 + 2 * 4) * fb + t_coef;
     }
+}
+}  // namespace bpk
+
+extern "C" {
+
+int bp_algorithmic_bytes(bp_sim* s, double bpc[2], long long* cells) {
+    if (!s || !bpc) { set_error("bad arguments"); return BP_ERR_ARG; }
+    algorithmic_bpc(s->shot.cfg, s->shot.med_tuples > 0, bpc);
     if (cells) *cells = s->shot.cells;
+    return BP_OK;
+}
+
+int bp_get_medium_tuples(bp_sim* s, int* ntuples) {
+    if (!s || !ntuples) { set_error("bad arguments"); return BP_ERR_ARG; }
+    *ntuples = s->shot.med_tuples;
     return BP_OK;
 }
 
@@ -583,8 +609,9 @@ int bp_profile_fused(bp_sim* s, int nsteps, float* ms, double* bytes_per_cell) {
         const bp_config& c = sh.cfg;
         const double fb = c.precision == BP_PREC_FP32 ? 4 : 3;
         const double cb = c.precision == BP_PREC_FP32 ? 4 : ((c.comp_coef_lo || c.precision == BP_PREC_CBF16) ? 3 : 2);
-        // 2D: the 8 fields read and written once, 7 V + 5 T coefficients read once
-        *bytes_per_cell = 2 * 8 * fb + 12 * cb;
+        // 2D: the 8 fields read and written once, 7 V + 5 T coefficients read
+        // once (an indexed medium: one index byte)
+        *bytes_per_cell = 2 * 8 * fb + (sh.med_tuples > 0 ? 1.0 : 12 * cb);
     }
     return BP_OK;
 }

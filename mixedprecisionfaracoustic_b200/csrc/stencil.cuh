@@ -233,6 +233,48 @@ struct TailOut {
     __device__ __forceinline__ static TailOut t_of(const ShotDesc& S) { return TailOut{S.f, S.flo, S.psiT, nullptr, true}; }
 };
 
+// Coefficients of a chunk: from the per-cell arrays, or from the tuple table
+// of an indexed medium (float policies only; FP64 shots are never indexed).
+template <class P>
+__device__ __forceinline__ bool med_on(const ShotDesc& S) {
+    if constexpr (sizeof(typename P::real) == 4) return S.med_idx != nullptr;
+    else return false;
+}
+// Component q of group g of the chunk's four tuples.
+template <class R>
+__device__ __forceinline__ void med_comp4(const ShotDesc& S, unsigned ids, int g, int q, R (&o)[4]) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const float4 t = med_group(S, ids, j, g);
+        o[j] = (R)(q == 0 ? t.x : q == 1 ? t.y : q == 2 ? t.z : t.w);
+    }
+}
+// One V-phase coefficient (VCoef k) of the chunk at c.
+template <class P, bool NC = kReadOnlyPath>
+__device__ __forceinline__ void vcoef4(const ShotDesc& S, int k, cidx c, typename P::real (&o)[4]) {
+    if (med_on<P>(S)) {
+        const int g = (k == VC_RHO_Y || k == VC_CC1_Y || k == VC_CC2_Y) ? MED_V_Y
+                      : (k == VC_RHO_Z || k == VC_CC1_Z || k == VC_CC2_Z) ? MED_V_Z : MED_V_X;
+        const int q = k == VC_RHOF ? 3 : (k == VC_RHO_X || k == VC_RHO_Y || k == VC_RHO_Z) ? 0
+                      : (k == VC_CC1_X || k == VC_CC1_Y || k == VC_CC1_Z) ? 1 : 2;
+        med_comp4(S, med_ids(S, c), g, q, o);
+        return;
+    }
+    P::template ld4<NC>(S.vc[k], S.vclo[k], c, o);
+}
+// One T-phase coefficient (TCoef k) of the chunk at c.
+template <class P, bool NC = kReadOnlyPath>
+__device__ __forceinline__ void tcoef4(const ShotDesc& S, int k, cidx c, typename P::real (&o)[4]) {
+    if (med_on<P>(S)) {
+        const int g = (k == TC_C || k == TC_M || k == TC_H || k == TC_H2U) ? MED_T_A : MED_T_B;
+        const int q = (k == TC_C || k == TC_MUXZ) ? 0 : (k == TC_M || k == TC_MUXY) ? 1
+                      : (k == TC_H || k == TC_MUYZ) ? 2 : 3;
+        med_comp4(S, med_ids(S, c), g, q, o);
+        return;
+    }
+    P::template ld4<NC>(S.tc[k], S.tclo[k], c, o);
+}
+
 template <class R>
 struct VState {
     R x1[4], x3[4], s1[4], z1[4], z2[4], s3[4];       // derivatives (2D and 3D)
@@ -252,11 +294,24 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y,
     auto &rf = V.rf, &rho_x = V.rho_x, &c1_x = V.c1_x, &c2_x = V.c2_x, &vu_x = V.vu_x, &vw_x = V.vw_x;
     auto &rho_z = V.rho_z, &c1_z = V.c1_z, &c2_z = V.c2_z, &vu_z = V.vu_z, &vw_z = V.vw_z;
     auto &rho_y = V.rho_y, &c1_y = V.c1_y, &c2_y = V.c2_y, &vu_y = V.vu_y, &vw_y = V.vw_y;
+    const bool med = med_on<P>(S);
     auto load_axis = [&](int fu, int fw, int crho, int ccc1, int ccc2, R (&rho)[4], R (&c1)[4], R (&c2)[4],
                          R (&vu)[4], R (&vw)[4]) {
-        P::template ld4<NC>(S.vc[crho], S.vclo[crho], c, rho);
-        P::template ld4<NC>(S.vc[ccc1], S.vclo[ccc1], c, c1);
-        P::template ld4<NC>(S.vc[ccc2], S.vclo[ccc2], c, c2);
+        if (med) {
+            // one group per cell: (rho, cc1, cc2, rhof) of this axis
+            const int g = crho == VC_RHO_X ? MED_V_X : crho == VC_RHO_Y ? MED_V_Y : MED_V_Z;
+            const unsigned ids = med_ids(S, c);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float4 t = med_group(S, ids, j, g);
+                rho[j] = (R)t.x; c1[j] = (R)t.y; c2[j] = (R)t.z;
+                if (g == MED_V_X) rf[j] = (R)t.w;
+            }
+        } else {
+            P::template ld4<NC>(S.vc[crho], S.vclo[crho], c, rho);
+            P::template ld4<NC>(S.vc[ccc1], S.vclo[ccc1], c, c1);
+            P::template ld4<NC>(S.vc[ccc2], S.vclo[ccc2], c, c2);
+        }
         P::ld4(S.f[fu], S.flo[fu], c, vu);
         P::ld4(S.f[fw], S.flo[fw], c, vw);
     };
@@ -356,7 +411,7 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y,
         for (int j = 0; j < 4; j++) { vw[j] = nw[j]; vu[j] = nu[j]; }
     };
     if constexpr (!PRE) {
-        P::template ld4<NC>(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, rf);
+        if (!med) P::template ld4<NC>(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, rf);   // indexed: with the x group
         load_axis(BP_F_VUX, BP_F_VWX, VC_RHO_X, VC_CC1_X, VC_CC2_X, rho_x, c1_x, c2_x, vu_x, vw_x);
     }
     axis_update(sumx, s1, BP_F_VUX, BP_F_VWX, rho_x, c1_x, c2_x, vu_x, vw_x);
@@ -398,18 +453,31 @@ __device__ __forceinline__ void t_tail(const ShotDesc& S, cidx c, int x0, int y,
     auto &op = T.op, &oxx = T.oxx, &ozz = T.ozz, &oxz = T.oxz;
     auto &mxy = T.mxy, &myz = T.myz, &oyy = T.oyy, &oxy = T.oxy, &oyz = T.oyz;
     auto load_state = [&]() {
-        P::template ld4<NC>(S.tc[TC_C], S.tclo[TC_C], c, cC);
-        P::template ld4<NC>(S.tc[TC_M], S.tclo[TC_M], c, cM);
-        P::template ld4<NC>(S.tc[TC_H], S.tclo[TC_H], c, cH);
-        P::template ld4<NC>(S.tc[TC_H2U], S.tclo[TC_H2U], c, cH2);
-        P::template ld4<NC>(S.tc[TC_MUXZ], S.tclo[TC_MUXZ], c, mxz);
+        if (med_on<P>(S)) {
+            const unsigned ids = med_ids(S, c);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float4 a = med_group(S, ids, j, MED_T_A);
+                const float4 b = med_group(S, ids, j, MED_T_B);
+                cC[j] = (R)a.x; cM[j] = (R)a.y; cH[j] = (R)a.z; cH2[j] = (R)a.w; mxz[j] = (R)b.x;
+                if constexpr (DIM == 3) { mxy[j] = (R)b.y; myz[j] = (R)b.z; }
+            }
+        } else {
+            P::template ld4<NC>(S.tc[TC_C], S.tclo[TC_C], c, cC);
+            P::template ld4<NC>(S.tc[TC_M], S.tclo[TC_M], c, cM);
+            P::template ld4<NC>(S.tc[TC_H], S.tclo[TC_H], c, cH);
+            P::template ld4<NC>(S.tc[TC_H2U], S.tclo[TC_H2U], c, cH2);
+            P::template ld4<NC>(S.tc[TC_MUXZ], S.tclo[TC_MUXZ], c, mxz);
+            if constexpr (DIM == 3) {
+                P::template ld4<NC>(S.tc[TC_MUXY], S.tclo[TC_MUXY], c, mxy);
+                P::template ld4<NC>(S.tc[TC_MUYZ], S.tclo[TC_MUYZ], c, myz);
+            }
+        }
         P::ld4(S.f[BP_F_P], S.flo[BP_F_P], c, op);
         P::ld4(S.f[BP_F_TXX], S.flo[BP_F_TXX], c, oxx);
         P::ld4(S.f[BP_F_TZZ], S.flo[BP_F_TZZ], c, ozz);
         P::ld4(S.f[BP_F_TXZ], S.flo[BP_F_TXZ], c, oxz);
         if constexpr (DIM == 3) {
-            P::template ld4<NC>(S.tc[TC_MUXY], S.tclo[TC_MUXY], c, mxy);
-            P::template ld4<NC>(S.tc[TC_MUYZ], S.tclo[TC_MUYZ], c, myz);
             P::ld4(S.f[BP_F_TYY], S.flo[BP_F_TYY], c, oyy);
             P::ld4(S.f[BP_F_TXY], S.flo[BP_F_TXY], c, oxy);
             P::ld4(S.f[BP_F_TYZ], S.flo[BP_F_TYZ], c, oyz);

@@ -170,6 +170,24 @@ __global__ void k_coef(const ShotDesc* __restrict__ shots, int which, float* out
 
 // ---------------------------------------------------------------------------
 // Host-side launchers (explicit instantiation over dim x order x precision).
+
+// Shared-memory carveout of the phase kernels, in percent of the SM's unified
+// L1/shared storage (their only shared data is the shot descriptor; the rest
+// serves as L1 for the neighbour re-reads); -1 leaves the driver's choice.
+#ifndef BP_L1_CARVEOUT
+#define BP_L1_CARVEOUT -1
+#endif
+template <int D, int O, class P, bool V, bool M>
+static void phase_carveout() {
+    if constexpr (BP_L1_CARVEOUT >= 0) {
+        static bool set = false;                       // once per kernel
+        if (!set) {
+            cudaFuncSetAttribute(k_phase<D, O, P, V, M>, cudaFuncAttributePreferredSharedMemoryCarveout, BP_L1_CARVEOUT);
+            set = true;
+        }
+    }
+}
+
 template <class P>
 struct Launch {
     static cudaError_t phase(int dim, int order, bool v, const ShotDesc* d_shots, int nshots, long long ntiles,
@@ -177,11 +195,15 @@ struct Launch {
 #define BPK_LAUNCH(D, O)                                                                                        \
     if (dim == D && order == O) {                                                                               \
         if (multi) {                                                                                            \
-            if (v) k_phase<D, O, P, true, true><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, 0);      \
-            else k_phase<D, O, P, false, true><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, post);    \
+            if (v) { phase_carveout<D, O, P, true, true>();                                                     \
+                     k_phase<D, O, P, true, true><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, 0); }  \
+            else { phase_carveout<D, O, P, false, true>();                                                      \
+                   k_phase<D, O, P, false, true><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, post); } \
         } else {                                                                                                \
-            if (v) k_phase<D, O, P, true, false><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, 0);     \
-            else k_phase<D, O, P, false, false><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, post);   \
+            if (v) { phase_carveout<D, O, P, true, false>();                                                    \
+                     k_phase<D, O, P, true, false><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, 0); } \
+            else { phase_carveout<D, O, P, false, false>();                                                     \
+                   k_phase<D, O, P, false, false><<<grid, kThreads, 0, st>>>(d_shots, nshots, ntiles, k, post); } \
         }                                                                                                       \
         return cudaGetLastError();                                                                              \
     }

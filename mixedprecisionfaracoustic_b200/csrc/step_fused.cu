@@ -213,15 +213,15 @@ __device__ __forceinline__ void fused_task(const ShotDesc& S, int it, typename P
             dz_win<ORD, P, true>(wp, 0, S, V.s3);                    // p: D+z
             if (act) {
                 const cidx c = at(z);
-                P::ld4(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, V.rf);
-                P::ld4(S.vc[VC_RHO_X], S.vclo[VC_RHO_X], c, V.rho_x);
-                P::ld4(S.vc[VC_CC1_X], S.vclo[VC_CC1_X], c, V.c1_x);
-                P::ld4(S.vc[VC_CC2_X], S.vclo[VC_CC2_X], c, V.c2_x);
+                vcoef4<P, false>(S, VC_RHOF, c, V.rf);
+                vcoef4<P, false>(S, VC_RHO_X, c, V.rho_x);
+                vcoef4<P, false>(S, VC_CC1_X, c, V.c1_x);
+                vcoef4<P, false>(S, VC_CC2_X, c, V.c2_x);
                 P::ld4(fi[BP_F_VUX], fli[BP_F_VUX], c, V.vu_x);
                 P::ld4(fi[BP_F_VWX], fli[BP_F_VWX], c, V.vw_x);
-                P::ld4(S.vc[VC_RHO_Z], S.vclo[VC_RHO_Z], c, V.rho_z);
-                P::ld4(S.vc[VC_CC1_Z], S.vclo[VC_CC1_Z], c, V.c1_z);
-                P::ld4(S.vc[VC_CC2_Z], S.vclo[VC_CC2_Z], c, V.c2_z);
+                vcoef4<P, false>(S, VC_RHO_Z, c, V.rho_z);
+                vcoef4<P, false>(S, VC_CC1_Z, c, V.c1_z);
+                vcoef4<P, false>(S, VC_CC2_Z, c, V.c2_z);
                 P::ld4(fi[BP_F_VUZ], fli[BP_F_VUZ], c, V.vu_z);
                 P::ld4(fi[BP_F_VWZ], fli[BP_F_VWZ], c, V.vw_z);
                 TailOut o = outV;
@@ -250,11 +250,11 @@ __device__ __forceinline__ void fused_task(const ShotDesc& S, int it, typename P
             dz_win<ORD, P, true>(vux, 1, S, T.uxz);                 // vux: D+z, rows q-HW+1 ..
             if (own) {                                              // the halo lanes' stresses are not needed
                 const cidx c = at(q);
-                P::ld4(S.tc[TC_C], S.tclo[TC_C], c, T.cC);
-                P::ld4(S.tc[TC_M], S.tclo[TC_M], c, T.cM);
-                P::ld4(S.tc[TC_H], S.tclo[TC_H], c, T.cH);
-                P::ld4(S.tc[TC_H2U], S.tclo[TC_H2U], c, T.cH2);
-                P::ld4(S.tc[TC_MUXZ], S.tclo[TC_MUXZ], c, T.mxz);
+                tcoef4<P, false>(S, TC_C, c, T.cC);
+                tcoef4<P, false>(S, TC_M, c, T.cM);
+                tcoef4<P, false>(S, TC_H, c, T.cH);
+                tcoef4<P, false>(S, TC_H2U, c, T.cH2);
+                tcoef4<P, false>(S, TC_MUXZ, c, T.mxz);
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     T.op[j] = wp[0][j]; T.oxx[j] = wxx[0][j]; T.ozz[j] = wzz[0][j]; T.oxz[j] = wxz[0][j];

@@ -435,9 +435,9 @@ __device__ __forceinline__ void v_comp(const ShotDesc& S, cidx c, cidx row, int 
     constexpr int cc1 = AX == 0 ? VC_CC1_X : AX == 1 ? VC_CC1_Y : VC_CC1_Z;
     constexpr int cc2 = AX == 0 ? VC_CC2_X : AX == 1 ? VC_CC2_Y : VC_CC2_Z;
     R rho[4], c1[4], c2[4], vu[4], vw[4], nu[4], nw[4];
-    P::template ld4<kReadOnlyPath>(S.vc[crho], S.vclo[crho], c, rho);
-    P::template ld4<kReadOnlyPath>(S.vc[cc1], S.vclo[cc1], c, c1);
-    P::template ld4<kReadOnlyPath>(S.vc[cc2], S.vclo[cc2], c, c2);
+    vcoef4<P>(S, crho, c, rho);
+    vcoef4<P>(S, cc1, c, c1);
+    vcoef4<P>(S, cc2, c, c2);
     P::ld4(S.f[fu], S.flo[fu], c, vu);
     P::ld4(S.f[fw], S.flo[fw], c, vw);
 #pragma unroll
@@ -468,7 +468,7 @@ __device__ __forceinline__ void v_chunk_g(const ShotDesc& S, int x0, int y, int 
     const cidx c = x0 + y * S.pitch + z * (cidx)S.plane;
     const cidx row = c - x0;
     R rf[4];
-    P::template ld4<kReadOnlyPath>(S.vc[VC_RHOF], S.vclo[VC_RHOF], c, rf);
+    vcoef4<P>(S, VC_RHOF, c, rf);
     v_comp<DIM, ORD, P, RS, 0>(S, c, row, x0, y, z, r, mask, rf);
     if constexpr (DIM == 3) v_comp<DIM, ORD, P, RS, 1>(S, c, row, x0, y, z, r, mask, rf);
     v_comp<DIM, ORD, P, RS, 2>(S, c, row, x0, y, z, r, mask, rf);
@@ -522,7 +522,7 @@ __device__ __forceinline__ void t_shear(const ShotDesc& S, cidx c, cidx row, int
     constexpr int f = SH == 0 ? BP_F_TXY : SH == 1 ? BP_F_TYZ : BP_F_TXZ;
     constexpr int cm = SH == 0 ? TC_MUXY : SH == 1 ? TC_MUYZ : TC_MUXZ;
     R mu[4], o[4], n[4];
-    P::template ld4<kReadOnlyPath>(S.tc[cm], S.tclo[cm], c, mu);
+    tcoef4<P>(S, cm, c, mu);
     ld_old<P, RS>(S, f, c, r, o);
     const R dt = S.dtr<R>();
 #pragma unroll
@@ -574,8 +574,8 @@ __device__ __forceinline__ void t_chunk_g(const ShotDesc& S, int x0, int y, int 
     }
     R cC[4], cM[4], cH[4], cH2[4], o[4], n[4];
     const R dt = S.dtr<R>();
-    P::template ld4<kReadOnlyPath>(S.tc[TC_C], S.tclo[TC_C], c, cC);
-    P::template ld4<kReadOnlyPath>(S.tc[TC_M], S.tclo[TC_M], c, cM);
+    tcoef4<P>(S, TC_C, c, cC);
+    tcoef4<P>(S, TC_M, c, cM);
     ld_old<P, RS>(S, BP_F_P, c, r, o);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -592,8 +592,8 @@ __device__ __forceinline__ void t_chunk_g(const ShotDesc& S, int x0, int y, int 
         }
     }
     st_new<P>(S, BP_F_P, c, mask, n, o);
-    P::template ld4<kReadOnlyPath>(S.tc[TC_H], S.tclo[TC_H], c, cH);
-    P::template ld4<kReadOnlyPath>(S.tc[TC_H2U], S.tclo[TC_H2U], c, cH2);
+    tcoef4<P>(S, TC_H, c, cH);
+    tcoef4<P>(S, TC_H2U, c, cH2);
     ld_old<P, RS>(S, BP_F_TXX, c, r, o);
 #pragma unroll
     for (int j = 0; j < 4; j++) {

@@ -98,6 +98,7 @@ def test_comp16_within_1e3_of_fp64(kind, order):
 def test_staged_kernels_match_oracle_and_register_kernels(prec, order):
     """The TMA-staged 2D phase kernels against the oracle and the register kernels."""
     cfg, med = small_2d(order, prec, nx=300, nz=70, nt=200)
+    cfg.medium = "dense"                 # the staged kernels read the per-cell coefficient arrays
     out = {}
     for variant in ("register", "staged"):
         with Simulation(cfg, med) as s:
@@ -119,6 +120,7 @@ def test_march_kernels_bit_identical_to_register_kernels(prec, order, nx, nz):
     width is, and is not, a multiple of the 128-cell column and whose height
     splits into several z segments; and within tolerance of the oracle."""
     cfg, med = small_2d(order, prec, nx=nx, nz=nz, nt=160)
+    cfg.medium = "dense"                 # the marching kernels read the per-cell coefficient arrays
     out = {}
     for variant in ("register", "march"):
         with Simulation(cfg, med) as s:
