@@ -150,11 +150,11 @@ static cudaError_t med_build(ShotDesc& S, uint8_t* d_idx, float4* d_tab, void* d
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return e;
     if (flags[1] || flags[0] > kMedMaxTuples || flags[0] < 1) return cudaSuccess;   // too many tuples: dense
-    std::vector<int> ids(kSlots, 0), rep_of(flags[0]);
+    std::vector<int> ids(kSlots, 0), rep_of(kSlots, 0);
     int n = 0;
     for (int s = 0; s < kSlots; s++)
         if (keys[s]) { ids[s] = n; rep_of[n] = reps[s]; n++; }
-    if (n != flags[0]) return cudaSuccess;
+    if (n != flags[0] || n > kMedMaxTuples) return cudaSuccess;
     int* d_reps = M->reps;                 // reused: rep of each tuple number, after the index pass
     e = cudaMemcpyAsync(M->ids, ids.data(), sizeof(M->ids), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
