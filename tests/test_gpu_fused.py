@@ -60,7 +60,13 @@ def test_fused_step_launch_count_and_profile():
         s.sync()
         assert s.launch_count() - l0 == 66
         ms, bpc = s.profile_fused(10)
-        assert ms > 0 and bpc == 2 * 8 * 4 + 12 * 4
+        # fields once each way, coefficients once: one index byte for the
+        # layered (indexed) medium, 12 words on the per-cell arrays
+        assert ms > 0 and bpc == 2 * 8 * 4 + (1 if s.medium_tuples() else 12 * 4)
+    cfg.medium = "dense"
+    with Simulation(cfg, med) as s:
+        s.set_kernel("fused")
+        assert s.profile_fused(4)[1] == 2 * 8 * 4 + 12 * 4
 
 
 def test_fused_refused_where_it_does_not_apply():
