@@ -151,6 +151,18 @@ __device__ __forceinline__ unsigned med_ids(const ShotDesc& S, cidx c) {
 __device__ __forceinline__ float4 med_group(const ShotDesc& S, unsigned ids, int j, int g) {
     return __ldg(S.ctab + ((ids >> (8 * j)) & 0xffu) * kMedRow + g);
 }
+// Group g of the chunk's four tuples: one load when the four cells share a
+// tuple (a layered medium's rows, the bulk of a blocky one), else four.
+__device__ __forceinline__ void med_group4(const ShotDesc& S, unsigned ids, int g, float4 (&t)[4]) {
+    const unsigned id0 = ids & 0xffu;
+    if (ids == id0 * 0x01010101u) {
+        const float4 u = __ldg(S.ctab + id0 * kMedRow + g);
+        t[0] = u; t[1] = u; t[2] = u; t[3] = u;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) t[j] = med_group(S, ids, j, g);
+    }
+}
 
 // Steps are issued in chunks; step k of a chunk of shot s has index
 // it = *step_base + k.  Reading the base from device memory lets one captured

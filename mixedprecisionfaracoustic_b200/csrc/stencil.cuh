@@ -243,11 +243,10 @@ __device__ __forceinline__ bool med_on(const ShotDesc& S) {
 // Component q of group g of the chunk's four tuples.
 template <class R>
 __device__ __forceinline__ void med_comp4(const ShotDesc& S, unsigned ids, int g, int q, R (&o)[4]) {
+    float4 t[4];
+    med_group4(S, ids, g, t);
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-        const float4 t = med_group(S, ids, j, g);
-        o[j] = (R)(q == 0 ? t.x : q == 1 ? t.y : q == 2 ? t.z : t.w);
-    }
+    for (int j = 0; j < 4; j++) o[j] = (R)(q == 0 ? t[j].x : q == 1 ? t[j].y : q == 2 ? t[j].z : t[j].w);
 }
 // One V-phase coefficient (VCoef k) of the chunk at c.
 template <class P, bool NC = kReadOnlyPath>
@@ -281,6 +280,7 @@ struct VState {
     R x2[4], y1[4], y2[4], y3[4], s2[4], z3[4];       // 3D only
     R rf[4], rho_x[4], c1_x[4], c2_x[4], vu_x[4], vw_x[4], rho_z[4], c1_z[4], c2_z[4], vu_z[4], vw_z[4];
     R rho_y[4], c1_y[4], c2_y[4], vu_y[4], vw_y[4];
+    unsigned mids;                 // indexed medium: the chunk's four tuple indices (set before the tail)
 };
 
 // On return V's old-velocity members (vu_*, vw_*) hold the new velocities as a
@@ -300,12 +300,12 @@ __device__ __forceinline__ void v_tail(const ShotDesc& S, cidx c, int x0, int y,
         if (med) {
             // one group per cell: (rho, cc1, cc2, rhof) of this axis
             const int g = crho == VC_RHO_X ? MED_V_X : crho == VC_RHO_Y ? MED_V_Y : MED_V_Z;
-            const unsigned ids = med_ids(S, c);
+            float4 t[4];
+            med_group4(S, V.mids, g, t);
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                const float4 t = med_group(S, ids, j, g);
-                rho[j] = (R)t.x; c1[j] = (R)t.y; c2[j] = (R)t.z;
-                if (g == MED_V_X) rf[j] = (R)t.w;
+                rho[j] = (R)t[j].x; c1[j] = (R)t[j].y; c2[j] = (R)t[j].z;
+                if (g == MED_V_X) rf[j] = (R)t[j].w;
             }
         } else {
             P::template ld4<NC>(S.vc[crho], S.vclo[crho], c, rho);
@@ -440,6 +440,7 @@ struct TState {
     R uyy[4], wy[4], uxy[4], uyx[4], uyz[4], uzy[4];   // 3D only
     R cC[4], cM[4], cH[4], cH2[4], mxz[4], op[4], oxx[4], ozz[4], oxz[4];
     R mxy[4], myz[4], oyy[4], oxy[4], oyz[4];
+    unsigned mids;                 // indexed medium: the chunk's four tuple indices (set before the tail)
 };
 
 // On return T's old-stress members (op, oxx, ...) hold the new values.
@@ -454,13 +455,14 @@ __device__ __forceinline__ void t_tail(const ShotDesc& S, cidx c, int x0, int y,
     auto &mxy = T.mxy, &myz = T.myz, &oyy = T.oyy, &oxy = T.oxy, &oyz = T.oyz;
     auto load_state = [&]() {
         if (med_on<P>(S)) {
-            const unsigned ids = med_ids(S, c);
+            const unsigned ids = T.mids;
+            float4 a[4], b[4];
+            med_group4(S, ids, MED_T_A, a);
+            med_group4(S, ids, MED_T_B, b);
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                const float4 a = med_group(S, ids, j, MED_T_A);
-                const float4 b = med_group(S, ids, j, MED_T_B);
-                cC[j] = (R)a.x; cM[j] = (R)a.y; cH[j] = (R)a.z; cH2[j] = (R)a.w; mxz[j] = (R)b.x;
-                if constexpr (DIM == 3) { mxy[j] = (R)b.y; myz[j] = (R)b.z; }
+                cC[j] = (R)a[j].x; cM[j] = (R)a[j].y; cH[j] = (R)a[j].z; cH2[j] = (R)a[j].w; mxz[j] = (R)b[j].x;
+                if constexpr (DIM == 3) { mxy[j] = (R)b[j].y; myz[j] = (R)b[j].z; }
             }
         } else {
             P::template ld4<NC>(S.tc[TC_C], S.tclo[TC_C], c, cC);
