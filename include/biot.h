@@ -307,6 +307,24 @@ int bp_profile_fused(bp_sim* sim, int nsteps, float* ms, double* bytes_per_cell)
  * numerator) and the number of updated cells per step.  An indexed medium
  * (BP_MEDIUM_AUTO) counts one index byte per phase for its coefficients. */
 int bp_algorithmic_bytes(bp_sim* sim, double bytes_per_cell[2], long long* cells);
+/* Variable grid along z (the depth axis).  dz[k], k = 0 .. n-1 with
+ * n = nz + 2 npml - 1, is the spacing in metres between padded z rows k and
+ * k+1; the z differences of the fields then divide by the local spacing: the
+ * forward difference of rows z, z+1 (giving the value at z + 1/2) by dz[z], the
+ * backward one of the half rows z - 1/2, z + 1/2 (giving the value at z) by
+ * (dz[z-1] + dz[z]) / 2; the x and y spacing stays dx.  No working
+ * counterpart in the reference: Float/main.cu:24-25 (NL, m) and :76-89 (h =
+ * H/m, h1 = h/m, ..., c1 = 2/(h + H), cc1 = 2/(h + h1), ...) define the
+ * constants of such a grid, a spacing that changes by a factor m at a depth,
+ * which no computation there uses; this entry point builds that scheme.
+ * FP32 with BP_ROUND_FAST at order 2, one shot (not batches or the server),
+ * the register tile kernels; the first and last npml + 1 spacings must equal
+ * dx (the CPML profiles are the uniform grid's).  Call once, before the first
+ * step; with check_cfl, dt is checked against the finest spacing
+ * (BP_ERR_CFL).  A checkpoint holds no spacing: set the same one on the
+ * simulation it is restored into. */
+int bp_set_z_spacing(bp_sim* sim, const double* dz, int n);
+
 /* Distinct coefficient tuples of an indexed medium, 0 where the shot reads
  * the per-cell coefficient arrays (BP_MEDIUM_DENSE, FP64, > 256 tuples). */
 int bp_get_medium_tuples(bp_sim* sim, int* ntuples);

@@ -98,6 +98,7 @@ _SIGS = [
     ("bp_algorithmic_bytes", C.c_int, [C.c_void_p, DoubleP, C.POINTER(C.c_longlong)]),
     ("bp_launches_per_step", C.c_int, [C.c_void_p, IntP]),
     ("bp_get_medium_tuples", C.c_int, [C.c_void_p, IntP]),
+    ("bp_set_z_spacing", C.c_int, [C.c_void_p, DoubleP, C.c_int]),
     ("bp_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     ("bp_comp16_encode", C.c_int, [FloatP, C.c_size_t, C.POINTER(C.c_uint16), C.POINTER(C.c_int8)]),
     ("bp_comp16_decode", C.c_int, [C.POINTER(C.c_uint16), C.POINTER(C.c_int8), C.c_size_t, FloatP]),

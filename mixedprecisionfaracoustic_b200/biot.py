@@ -294,6 +294,12 @@ class Simulation:
         check(self.lib.bp_get_medium_tuples(self.h, C.byref(n)), "bp_get_medium_tuples")
         return n.value
 
+    def set_z_spacing(self, dz) -> None:
+        """Variable grid along z: dz[k] = spacing (m) between padded rows k and
+        k+1, nz + 2 npml - 1 values; FP32, order 2, before the first step."""
+        d = np.ascontiguousarray(dz, dtype=np.float64)
+        check(self.lib.bp_set_z_spacing(self.h, d.ctypes.data_as(_abi.DoubleP), d.size), "bp_set_z_spacing")
+
     def launches_per_step(self) -> int:
         """Kernels one step launches: 3, or 2 where the T phase records the
         receivers and injects the source itself."""

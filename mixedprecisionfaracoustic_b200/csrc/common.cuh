@@ -133,6 +133,9 @@ struct ShotDesc {
     const uint8_t* med_idx;
     const float4* ctab;
     int med_tuples, pad_med;
+    // variable grid along z (PolF32G): fwd factors of rows 0..nz-1, then bwd
+    // factors; null on a uniform grid
+    const float* zf;
     template <class R>
     __device__ __forceinline__ R dtr() const { return sizeof(R) == 8 ? (R)dtd : (R)dt; }
 };
@@ -225,6 +228,7 @@ struct PolF32 {
     static constexpr int prec = BP_PREC_FP32;
     static constexpr int store = BP_PREC_FP32;   // storage format (PolB24: BP_PREC_CBF16)
     static constexpr bool exact = false;      // reference rounding (PolF32R)
+    static constexpr bool graded = false;     // variable z spacing (PolF32G)
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
         float4 t = ldv<NC>(reinterpret_cast<const float4*>(static_cast<const float*>(p) + i));
@@ -266,6 +270,7 @@ struct PolF64 {
     static constexpr int prec = BP_PREC_FP64;
     static constexpr int store = BP_PREC_FP64;
     static constexpr bool exact = false;
+    static constexpr bool graded = false;
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
         const double2* q = reinterpret_cast<const double2*>(static_cast<const double*>(p) + i);
@@ -314,6 +319,14 @@ struct PolF64 {
 // double sum to float).  Same storage as PolF32.
 struct PolF32R : PolF32 {
     static constexpr bool exact = true;
+};
+
+// FP32 on a variable grid along z (bp_set_z_spacing): the z differences are
+// multiplied by per-row factors, fwd[z] = 1/dz[z] for the forward difference
+// from rows z, z+1 and bwd[z] = 2/(dz[z-1] + dz[z]) for the backward one from
+// the half rows z-1/2, z+1/2 (S.zf); x and y differences as PolF32.
+struct PolF32G : PolF32 {
+    static constexpr bool graded = true;
 };
 
 // Compensated BF16 storage (BP_PREC_CBF16): each value is the top 24 bits of
@@ -381,6 +394,7 @@ struct PolC16 {
     static constexpr int prec = BP_PREC_COMP16;
     static constexpr int store = BP_PREC_COMP16;
     static constexpr bool exact = false;
+    static constexpr bool graded = false;
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t* lo, cidx i, real (&v)[4]) {
         uint2 h = ldv<NC>(reinterpret_cast<const uint2*>(static_cast<const __half*>(p) + i));

@@ -33,6 +33,7 @@ struct Runner {
     int rounding = BP_ROUND_FAST;      // FP32 BP_ROUND_REFERENCE: PolF32R register kernels only
     bool multi_unit = false;           // the shots' tile shape has more units than a CTA has warps
     bool indexed = false;              // some shot reads an indexed medium (not the marching or staged kernels)
+    bool graded = false;               // a variable z grid (PolF32G register kernels only)
     long long ntiles_f = 0;            // tasks of the fused step kernel (0: some shot cannot take it)
     int grid_f = 1;
     bool fused = false;
@@ -75,6 +76,7 @@ struct Runner {
         reset_graph();
     }
     void select_kernels() {
+        if (graded) { fused = inter = march = staged = false; return; }
         const bool can_f = fused_supported(prec, dim) && ntiles_f > 0 && rounding == BP_ROUND_FAST;
         fused = can_f && (variant == BP_KERNEL_FUSED || (variant == BP_KERNEL_AUTO && fused_default()));
         const bool can_i = nitems_i > 0 && d_ctl && d_err && !multi_unit;
@@ -118,7 +120,7 @@ struct Runner {
         if (march) return launch_phase_march(prec, order, v, d_shots, nshots, ntiles_m, k, st);
         if (staged) return launch_phase_staged(prec, order, v, d_shots, nshots, ntiles_s, k, grid_s, d_err, st);
         return launch_phase(prec, dim, order, v, d_shots, nshots, ntiles, k, v ? grid_v : grid_t, st,
-                            (!v && fused_post()) ? 1 : 0, rounding, multi_unit);
+                            (!v && fused_post()) ? 1 : 0, rounding, multi_unit, graded);
     }
 
     // One step (index k of the chunk) of the two-phase kernels, or of the

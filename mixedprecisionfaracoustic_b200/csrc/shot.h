@@ -18,7 +18,7 @@ namespace bpk {
 // tile shape has more (row, segment) units than a CTA has warps
 cudaError_t launch_phase(int prec, int dim, int order, bool vphase, const ShotDesc* d_shots, int nshots,
                          long long ntiles, int k, int grid, cudaStream_t st, int post = 0, int rounding = 0,
-                         bool multi = false);
+                         bool multi = false, bool graded = false);
 cudaError_t launch_post(int prec, const ShotDesc* d_shots, int nshots, int max_rec, int k, int do_record,
                         cudaStream_t st);
 cudaError_t launch_inject(int prec, const ShotDesc* d_shots, int nshots, int k, cudaStream_t st);

@@ -21,6 +21,9 @@ struct bp_sim {
     Runner run;
     cudaStream_t st = nullptr;
     int device = 0;
+    double cfl_dtmax = 0;          // the stability limit found at create (check_cfl), 0 = not checked
+    float* d_zf = nullptr;         // variable z grid: the factor tables (arena cache)
+    size_t d_zf_bytes = 0;
 };
 
 #define SIM_CK(call)                                                                       \
@@ -141,6 +144,7 @@ int bp_create(const bp_config* cfg, const bp_medium* medium, bp_sim** out) {
     rc = s->shot.create(cfg, medium, s->st);
     const int crc = cfl_verdict(rc == BP_OK);
     if (!rc && crc) { cudaStreamSynchronize(s->st); rc = crc; }
+    s->cfl_dtmax = cfg->check_cfl && medium ? dtmax : 0.0;
     if (rc) { s->shot.destroy(); cudaStreamDestroy(s->st); delete s; return rc; }
     s->run.post_in_t = s->shot.post_in_t;
     s->run.rounding = cfg->rounding;
@@ -240,6 +244,10 @@ int bp_set_kernel(bp_sim* s, int variant) {
     }
     if (variant == BP_KERNEL_INTERLEAVED && (s->shot.nitems_i <= 0 || !s->run.d_ctl || !s->run.d_err)) {
         set_error("the interleaved step kernel has no control block for this simulation");
+        return BP_ERR_ARG;
+    }
+    if (s->run.graded && variant != BP_KERNEL_AUTO && variant != BP_KERNEL_REGISTER) {
+        set_error("a variable z grid runs the register tile kernels only");
         return BP_ERR_ARG;
     }
     if ((variant == BP_KERNEL_STAGED || variant == BP_KERNEL_MARCH) && s->shot.med_tuples > 0) {
@@ -651,8 +659,54 @@ void bp_destroy(bp_sim* s) {
     if (s->st) cudaStreamSynchronize(s->st);
     s->run.reset_graph();
     s->shot.destroy();
+    if (s->d_zf) arena_release(s->d_zf, s->d_zf_bytes);
     if (s->st) cudaStreamDestroy(s->st);
     delete s;
+}
+
+int bp_set_z_spacing(bp_sim* s, const double* dz, int n) {
+    if (!s || !dz) { set_error("bad arguments"); return BP_ERR_ARG; }
+    Shot& sh = s->shot;
+    const bp_config& c = sh.cfg;
+    if (c.precision != BP_PREC_FP32 || c.rounding != BP_ROUND_FAST || c.order != 2) {
+        set_error("the variable z grid runs FP32 with fast rounding at order 2");
+        return BP_ERR_ARG;
+    }
+    if (sh.it_host != 0 || s->d_zf) { set_error("set the z spacing once, before the first step"); return BP_ERR_STATE; }
+    const int nzp = sh.desc.nz;
+    if (n != nzp - 1) { set_error("dz needs nz + 2 npml - 1 spacings"); return BP_ERR_ARG; }
+    const double H = (double)c.dx;
+    double dmin = H;
+    for (int k = 0; k < n; k++) {
+        if (!(dz[k] > 0) || !std::isfinite(dz[k])) { set_error("spacings must be positive and finite"); return BP_ERR_ARG; }
+        const bool cpml_row = k < c.npml + 1 || k >= n - (c.npml + 1);
+        if (cpml_row && dz[k] != H) { set_error("the CPML rows keep the spacing dx"); return BP_ERR_ARG; }
+        dmin = std::min(dmin, dz[k]);
+    }
+    if (s->cfl_dtmax > 0 && (double)c.dt > s->cfl_dtmax * (dmin / H)) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "dt=%g exceeds the stability limit %g of the finest spacing %g", (double)c.dt,
+                 s->cfl_dtmax * (dmin / H), dmin);
+        set_error(buf);
+        return BP_ERR_CFL;
+    }
+    // fwd[z] = 1/dz[z]; bwd[z] = 2/(dz[z-1] + dz[z]); rows without both
+    // neighbours (never updated) take 1/dx
+    std::vector<float> zf(2 * (size_t)nzp);
+    for (int z = 0; z < nzp; z++) {
+        zf[z] = (float)(z < n ? 1.0 / dz[z] : 1.0 / H);
+        zf[nzp + z] = (float)((z >= 1 && z < n) ? 2.0 / (dz[z - 1] + dz[z]) : 1.0 / H);
+    }
+    SIM_CK(cudaSetDevice(s->device));
+    SIM_CK(cudaStreamSynchronize(s->st));
+    SIM_CK(arena_alloc(zf.size() * 4, (void**)&s->d_zf, &s->d_zf_bytes));
+    SIM_CK(cudaMemcpy(s->d_zf, zf.data(), zf.size() * 4, cudaMemcpyHostToDevice));
+    sh.desc.zf = s->d_zf;
+    SIM_CK(cudaMemcpy((void*)sh.d_desc, &sh.desc, sizeof(ShotDesc), cudaMemcpyHostToDevice));
+    s->run.graded = true;
+    s->run.select_kernels();
+    s->run.reset_graph();
+    return BP_OK;
 }
 
 // ---- reference-format text output (Float/main.cu:1501-1516,1563-1588) ----

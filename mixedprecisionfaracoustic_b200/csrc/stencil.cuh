@@ -26,6 +26,15 @@ __device__ __forceinline__ typename P::real deriv_div(typename P::real a, const 
     } else return a * S.inv_h;
 }
 
+// A difference along z divided by the row spacing: H on a uniform grid
+// (deriv_div), the row's factor on a variable one (PolF32G; FWD: the forward
+// difference of rows z, z+1, else the backward one of rows z-1, z).
+template <class P, bool FWD>
+__device__ __forceinline__ typename P::real deriv_z(typename P::real a, const ShotDesc& S, int z) {
+    if constexpr (P::graded) return __fmul_rn(a, S.zf[FWD ? z : S.nz + z]);   // never contracted into a later add
+    else return deriv_div<P>(a, S);
+}
+
 // Staggered difference from a span v[j] = f(x0 - HW + j).
 template <int ORD, class R>
 __device__ __forceinline__ R dfwd(const R* v, int j) {   // at x0+j+1/2

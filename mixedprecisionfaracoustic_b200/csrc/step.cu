@@ -207,7 +207,11 @@ struct Launch {
         }                                                                                                       \
         return cudaGetLastError();                                                                              \
     }
-        BPK_LAUNCH(2, 2) BPK_LAUNCH(2, 4) BPK_LAUNCH(3, 2) BPK_LAUNCH(3, 4)
+        if constexpr (P::graded) {           // the variable z grid: order 2 only
+            BPK_LAUNCH(2, 2) BPK_LAUNCH(3, 2)
+        } else {
+            BPK_LAUNCH(2, 2) BPK_LAUNCH(2, 4) BPK_LAUNCH(3, 2) BPK_LAUNCH(3, 4)
+        }
 #undef BPK_LAUNCH
         return cudaErrorInvalidValue;
     }
@@ -218,7 +222,12 @@ struct Launch {
 // C++ entry points used by the host code (sim.cu, batch.cu).
 namespace bpk {
 cudaError_t launch_phase(int prec, int dim, int order, bool vphase, const ShotDesc* d_shots, int nshots,
-                         long long ntiles, int k, int grid, cudaStream_t st, int post, int rounding, bool multi) {
+                         long long ntiles, int k, int grid, cudaStream_t st, int post, int rounding, bool multi,
+                         bool graded) {
+    if (graded) {
+        if (prec != BP_PREC_FP32 || rounding != BP_ROUND_FAST || order != 2) return cudaErrorInvalidValue;
+        return Launch<PolF32G>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
+    }
     if (prec == BP_PREC_FP32 && rounding == BP_ROUND_REFERENCE)
         return Launch<PolF32R>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
     if (prec == BP_PREC_FP32)

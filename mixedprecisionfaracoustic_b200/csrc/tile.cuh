@@ -164,19 +164,19 @@ __device__ __forceinline__ void v_chunk(const ShotDesc& S, int x0, int y, int z,
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
-            x3[j] = deriv_div<P>(rbwd<ORD>(t), S); }
+            x3[j] = deriv_z<P, false>(rbwd<ORD>(t), S, z); }
         load_rows<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TZZ], S.flo[BP_F_TZZ], c, sz, a);               // tzz: D+z
 #pragma unroll
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
-            z1[j] = deriv_div<P>(rfwd<ORD>(t), S); }
+            z1[j] = deriv_z<P, true>(rfwd<ORD>(t), S, z); }
         load_rows<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_P], S.flo[BP_F_P], c, sz, a);                   // p: D+z
 #pragma unroll
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
-            s3[j] = deriv_div<P>(rfwd<ORD>(t), S); }
+            s3[j] = deriv_z<P, true>(rfwd<ORD>(t), S, z); }
         if constexpr (DIM == 3) {
             load_span<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TXY], S.flo[BP_F_TXY], row, x0, S.nx, v);   // txy: D-x
 #pragma unroll
@@ -198,7 +198,7 @@ __device__ __forceinline__ void v_chunk(const ShotDesc& S, int x0, int y, int z,
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
                 for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
-                y3[j] = deriv_div<P>(rbwd<ORD>(t), S); }
+                y3[j] = deriv_z<P, false>(rbwd<ORD>(t), S, z); }
             load_rows<ORD, P, (read_only_loads<DIM, P, true>() && NCOK)>(S.f[BP_F_TYZ], S.flo[BP_F_TYZ], c, sy, a);           // tyz: D-y
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
@@ -248,19 +248,19 @@ __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z,
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
-            uzz[j] = deriv_div<P>(rbwd<ORD>(t), S); }
+            uzz[j] = deriv_z<P, false>(rbwd<ORD>(t), S, z); }
         load_rows<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VWZ], S.flo[BP_F_VWZ], c, sz, a);               // vwz: D-z
 #pragma unroll
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
-            wz[j] = deriv_div<P>(rbwd<ORD>(t), S); }
+            wz[j] = deriv_z<P, false>(rbwd<ORD>(t), S, z); }
         load_rows<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUX], S.flo[BP_F_VUX], c, sz, a);               // vux: D+z
 #pragma unroll
         for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
             for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
-            uxz[j] = deriv_div<P>(rfwd<ORD>(t), S); }
+            uxz[j] = deriv_z<P, true>(rfwd<ORD>(t), S, z); }
         if constexpr (DIM == 3) {
             load_span<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUY], S.flo[BP_F_VUY], row, x0, S.nx, v);   // vuy: D+x
 #pragma unroll
@@ -288,7 +288,7 @@ __device__ __forceinline__ void t_chunk(const ShotDesc& S, int x0, int y, int z,
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
 #pragma unroll
                 for (int k = 0; k <= ORD; k++) t[k] = a[k][j];
-                uyz[j] = deriv_div<P>(rfwd<ORD>(t), S); }
+                uyz[j] = deriv_z<P, true>(rfwd<ORD>(t), S, z); }
             load_rows<ORD, P, (read_only_loads<DIM, P, false>() && NCOK)>(S.f[BP_F_VUZ], S.flo[BP_F_VUZ], c, sy, a);           // vuz: D+y
 #pragma unroll
             for (int j = 0; j < 4; j++) { R t[ORD + 1];
@@ -353,6 +353,7 @@ __device__ __forceinline__ void d_span(const ShotDesc& S, int f, cidx row, int x
 template <int ORD, class P, bool FWD>
 __device__ __forceinline__ void d_rows(const ShotDesc& S, int f, cidx c, cidx stride,
                                        typename P::real (&d)[4]) {
+    static_assert(!P::graded, "the grouped forms take a uniform grid (FP32 runs the whole-chunk form)");
     using R = typename P::real;
     R a[ORD + 1][4];
     load_rows<ORD, P>(S.f[f], S.flo[f], c, stride, a);

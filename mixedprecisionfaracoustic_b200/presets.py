@@ -308,3 +308,15 @@ def config4_requests(seed: int = 4, n: int = 1000, precision: str = "fp32", scal
                              rec_x=rx, rec_y=[0] * nrec, rec_z=[npml + 2] * nrec)
             reqs.append((cfg, build if lazy else build()))
     return reqs
+
+
+def z_spacing_step(cfg: ShotConfig, z_fine: int, z_coarse: int, ratio: float) -> np.ndarray:
+    """Spacings of a variable z grid (bp_set_z_spacing) shaped like the
+    reference's unused variable-grid constants (Float/main.cu:24-25,76-89: the
+    spacing H drops by a factor m at a depth): dx down to padded row z_fine,
+    dx / ratio between rows z_fine and z_coarse, dx below; z_fine and z_coarse
+    must leave the CPML rows at dx.  Returns nz + 2 npml - 1 spacings."""
+    nzp = cfg.padded[2]
+    dz = np.full(nzp - 1, float(np.float32(cfg.dx)), dtype=np.float64)
+    dz[z_fine:z_coarse] /= ratio
+    return dz

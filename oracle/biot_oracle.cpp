@@ -157,6 +157,10 @@ struct Oracle {
     std::vector<T> cC, cM, cH, cH2u, muxy, muxz, muyz;
     std::vector<T> psiV[12], prevV[12], psiT[12], prevT[12];
     Profile prof[3];
+    // variable grid along z (order 2): per row the forward factor 1/dz[z] and
+    // the backward factor 2/(dz[z-1] + dz[z]); REF32 keeps them as floats
+    // (the GPU path's tables), FP64 as doubles; empty on a uniform grid
+    std::vector<T> zfw, zbw;
 
     std::vector<int> rec_idx;
     std::vector<float> traces;       // [comp][rec][nt]
@@ -323,6 +327,25 @@ struct Oracle {
         if (FWD) return (c1 * (a[i + st] - a[i]) + c2 * (a[i + 2 * st] - a[i - st])) / h;
         return (c1 * (a[i] - a[i - st]) + c2 * (a[i + st] - a[i - 2 * st])) / h;
     }
+    // z difference at row z: D<ORD, FWD> along sz on a uniform grid, else the
+    // order-2 difference times the row's factor (no counterpart in the
+    // reference, whose variable-grid constants h, h1.., c1 = 2/(h + H) of
+    // Float/main.cu:24-25,76-89 are never used)
+    template <int ORD, bool FWD>
+    inline T Dz(const T* a, size_t i, int z) const {
+        if (zfw.empty()) return D<ORD, FWD>(a, i, sz);
+        return FWD ? (a[i + sz] - a[i]) * zfw[z] : (a[i] - a[i - sz]) * zbw[z];
+    }
+    void set_z_spacing(const double* dz, int n) {
+        zfw.assign(nz, T(0));
+        zbw.assign(nz, T(0));
+        for (int z = 0; z < nz; z++) {
+            const double fw = z < n ? 1.0 / dz[z] : 1.0 / Hd;
+            const double bw = (z >= 1 && z < n) ? 2.0 / (dz[z - 1] + dz[z]) : 1.0 / Hd;
+            zfw[z] = REF ? (T)(float)fw : (T)fw;
+            zbw[z] = REF ? (T)(float)bw : (T)bw;
+        }
+    }
     // FD_V restated (Float/main.cu:103-191) for one row of cells
     template <int DIM, int ORD>
     void v_row(int y, int z) {
@@ -338,11 +361,11 @@ struct Oracle {
         for (int x = hw; x < nx - hw; x++) {
             const size_t i = base + x;
             T x1 = D<ORD, true>(txx, i, 1), s1 = D<ORD, true>(pp, i, 1), z2 = D<ORD, false>(txz, i, 1);
-            T x3 = D<ORD, false>(txz, i, sz), z1 = D<ORD, true>(tzz, i, sz), s3 = D<ORD, true>(pp, i, sz);
+            T x3 = Dz<ORD, false>(txz, i, z), z1 = Dz<ORD, true>(tzz, i, z), s3 = Dz<ORD, true>(pp, i, z);
             T x2 = 0, y1 = 0, y2 = 0, y3 = 0, z3 = 0, s2 = 0;
             if (DIM == 3) {
                 x2 = D<ORD, false>(txy, i, sy); y1 = D<ORD, true>(tyy, i, sy); y2 = D<ORD, false>(txy, i, 1);
-                y3 = D<ORD, false>(tyz, i, sz); z3 = D<ORD, false>(tyz, i, sy); s2 = D<ORD, true>(pp, i, sy);
+                y3 = Dz<ORD, false>(tyz, i, z); z3 = D<ORD, false>(tyz, i, sy); s2 = D<ORD, true>(pp, i, sy);
             }
             if (px.act2[x]) {
                 x1 = cpml(psiV[0][i], prevV[0][i], x1, 0, 1, x);
@@ -423,11 +446,11 @@ struct Oracle {
         for (int x = hw; x < nx - hw; x++) {
             const size_t i = base + x;
             T uxx = D<ORD, false>(vux, i, 1), wx = D<ORD, false>(vwx, i, 1), uzx = D<ORD, true>(vuz, i, 1);
-            T uzz = D<ORD, false>(vuz, i, sz), wz = D<ORD, false>(vwz, i, sz), uxz = D<ORD, true>(vux, i, sz);
+            T uzz = Dz<ORD, false>(vuz, i, z), wz = Dz<ORD, false>(vwz, i, z), uxz = Dz<ORD, true>(vux, i, z);
             T uyy = 0, wy = 0, uxy = 0, uyx = 0, uyz = 0, uzy = 0;
             if (DIM == 3) {
                 uyy = D<ORD, false>(vuy, i, sy); wy = D<ORD, false>(vwy, i, sy); uxy = D<ORD, true>(vux, i, sy);
-                uyx = D<ORD, true>(vuy, i, 1); uyz = D<ORD, true>(vuy, i, sz); uzy = D<ORD, true>(vuz, i, sy);
+                uyx = D<ORD, true>(vuy, i, 1); uyz = Dz<ORD, true>(vuy, i, z); uzy = D<ORD, true>(vuz, i, sy);
             }
             if (px.act[x]) {
                 uxx = cpml(psiT[0][i], prevT[0][i], uxx, 0, 0, x);
@@ -829,6 +852,18 @@ int orc_get_profile(void* hv, int axis, int which, double* out, size_t n) {
                 default: out[i] = p.ed2[i]; break;
             }
         }
+    });
+    return rc;
+}
+
+// Variable grid along z: dz[k] = spacing between padded rows k and k+1
+// (n = nz_padded - 1), order 2 only.
+int orc_set_z_spacing(void* hv, const double* dz, int n) {
+    Handle* h = (Handle*)hv;
+    int rc = 0;
+    ORC_DISPATCH(h, {
+        if (o->order != 2 || n != o->nz - 1) rc = 1;
+        else o->set_z_spacing(dz, n);
     });
     return rc;
 }

@@ -39,6 +39,7 @@ def load():
         lib.orc_get_coef.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.c_size_t]
         lib.orc_get_profile.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_size_t]
         lib.orc_get_step.argtypes = [C.c_void_p]
+        lib.orc_set_z_spacing.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
         lib.orc_destroy.argtypes = [C.c_void_p]
         lib.orc_set_threads.argtypes = [C.c_int]
         lib.orc_medium_reference_borehole.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float)]
@@ -93,6 +94,11 @@ class Oracle:
 
     def run(self, n: int) -> None:
         self.lib.orc_run(self.h, int(n))
+
+    def set_z_spacing(self, dz) -> None:
+        """Variable grid along z: dz[k] = spacing between padded rows k, k+1."""
+        d = np.ascontiguousarray(dz, dtype=np.float64)
+        assert self.lib.orc_set_z_spacing(self.h, _d(d), d.size) == 0
 
     @property
     def step(self) -> int:

@@ -129,3 +129,33 @@ def test_ref32_close_to_fp64(dim, order):
         x, y = a.traces(comp), b.traces(comp)
         assert np.abs(y).max() > 0
         assert np.linalg.norm(x - y) / np.linalg.norm(y) < 1e-5
+
+
+def test_oracle_variable_z_grid():
+    """The oracle's variable z grid: every spacing dx reproduces the uniform
+    grid (FP64 to rounding; REF32 within an ulp per difference, since it
+    multiplies by 1/dx where the uniform path divides by dx), and a refined
+    band changes the wavefield."""
+    import numpy as np
+    from mixedprecisionfaracoustic_b200.presets import config1, z_spacing_step
+    cfg, med = config1(precision="fp32", nx=60, nz=50, nt=120, npml=6, order=2, nrec=16, host=True)
+    cfg.dt = float(np.float32(cfg.dt / 2))
+    flat = np.full(cfg.padded[2] - 1, float(np.float32(cfg.dx)))
+    fine = z_spacing_step(cfg, 8, 40, 2.0)          # the source and receivers' rows lie in the band
+
+    def run(mode, dz):
+        o = O.Oracle(cfg, med, mode)
+        if dz is not None:
+            o.set_z_spacing(dz)
+        o.run(cfg.nt)
+        t = o.traces("txx").astype(np.float64)
+        o.close()
+        return t
+
+    def rel(a, b):
+        return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+    base64, base32 = run(O.FP64, None), run(O.REF32, None)
+    assert rel(run(O.FP64, flat), base64) <= 1e-12
+    assert rel(run(O.REF32, flat), base32) <= 1e-6
+    assert rel(run(O.FP64, fine), base64) >= 1e-3
