@@ -85,3 +85,15 @@ def test_host_builder_is_bit_identical_to_the_library():
     assert a.pml_v0 == b.pml_v0
     for k in ma:
         assert np.array_equal(ma[k], mb[k]), k
+
+
+def test_z_spacing_step():
+    """The variable z grid helper: dx outside the band, dx / ratio inside, the
+    CPML rows untouched, one spacing per pair of padded rows."""
+    import numpy as np
+    from mixedprecisionfaracoustic_b200.presets import config1, z_spacing_step
+    cfg, _ = config1(precision="fp32", nx=40, nz=50, nt=4, npml=6, nrec=4, host=True)
+    dz = z_spacing_step(cfg, 10, 30, 4.0)
+    assert dz.shape == (cfg.padded[2] - 1,)
+    assert np.all(dz[:10] == np.float32(cfg.dx)) and np.all(dz[30:] == np.float32(cfg.dx))
+    assert np.allclose(dz[10:30], np.float32(cfg.dx) / 4.0)
