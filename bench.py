@@ -607,15 +607,26 @@ def run_serve(args, rank):
     reqs = config4_requests(seed=4, n=args.requests, precision=args.precision, scale=args.scale, lazy=True)
     work = sum((c.padded[0] - 2) * max(c.padded[1] - 2, 1) * (c.padded[2] - 2) * c.nt for c, _ in reqs)
     srv = Server(hbm_budget_bytes=150 << 30, steps_per_sync=100, device=dev)
-    # capacity probe: the first 8 requests back to back
-    t0 = time.perf_counter()
-    probe = [srv.submit(c, m()) for c, m in reqs[:8]]
-    for r in probe:
-        srv.wait(r, 3600)
-    cap = sum((c.padded[0] - 2) * max(c.padded[1] - 2, 1) * (c.padded[2] - 2) * c.nt for c, _ in reqs[:8]) / (
-        time.perf_counter() - t0)
-    for r in probe:
-        srv.release(r)
+    # capacity probe: the first 6 2D and the first 2 3D requests, each class
+    # back to back, and the stream's capacity as the work-weighted harmonic
+    # mean of the two (a probe of the first 8 alone, mostly 2D, overstated the
+    # capacity of a stream whose work is mostly 3D)
+    def cells_of(c):
+        return (c.padded[0] - 2) * max(c.padded[1] - 2, 1) * (c.padded[2] - 2) * c.nt
+    cap_of = {}
+    for dim, k in ((2, 6), (3, 2)):
+        sample = [(c, m) for c, m in reqs if c.dim == dim][:k]
+        if not sample:
+            continue
+        t0 = time.perf_counter()
+        probe = [srv.submit(c, m()) for c, m in sample]
+        for r in probe:
+            srv.wait(r, 3600)
+        cap_of[dim] = sum(cells_of(c) for c, _ in sample) / (time.perf_counter() - t0)
+        for r in probe:
+            srv.release(r)
+    work_of = {d: sum(cells_of(c) for c, _ in reqs if c.dim == d) for d in cap_of}
+    cap = sum(work_of.values()) / sum(work_of[d] / cap_of[d] for d in cap_of)
     rate = 0.8 * cap / (work / len(reqs))         # requests per second at 80% of capacity
     rng = np.random.default_rng(4)
     gaps = rng.exponential(1.0 / rate, len(reqs))
@@ -645,7 +656,8 @@ def run_serve(args, rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "fp32" else "f16+i8 storage, f32 math", "data": "synthetic",
             "config": {"workload": f"c4: {len(reqs)} Poisson requests x{args.scale} size, {args.precision}",
-                       "rate_per_s": rate, "capacity_cell_updates_per_s": cap, "hbm_budget_GB": 150},
+                       "rate_per_s": rate, "capacity_cell_updates_per_s": cap,
+                       "capacity_probe": {f"{d}d": v for d, v in cap_of.items()}, "hbm_budget_GB": 150},
             "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
             "server": {k: st[k] for k in ("completed", "max_resident", "busy_seconds", "cell_updates")},
             "clocks": clk.summary(), "elapsed_s": el, "requests_3d": sum(1 for c, _ in reqs if c.dim == 3),
