@@ -229,6 +229,7 @@ struct PolF32 {
     static constexpr int store = BP_PREC_FP32;   // storage format (PolB24: BP_PREC_CBF16)
     static constexpr bool exact = false;      // reference rounding (PolF32R)
     static constexpr bool graded = false;     // variable z spacing (PolF32G)
+    static constexpr bool wide = false;       // 3D register caps for large grids (PolF32W)
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
         float4 t = ldv<NC>(reinterpret_cast<const float4*>(static_cast<const float*>(p) + i));
@@ -270,6 +271,7 @@ struct PolF64 {
     static constexpr int prec = BP_PREC_FP64;
     static constexpr int store = BP_PREC_FP64;
     static constexpr bool exact = false;
+    static constexpr bool wide = false;
     static constexpr bool graded = false;
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t*, cidx i, real (&v)[4]) {
@@ -327,6 +329,12 @@ struct PolF32R : PolF32 {
 // the half rows z-1/2, z+1/2 (S.zf); x and y differences as PolF32.
 struct PolF32G : PolF32 {
     static constexpr bool graded = true;
+};
+
+// FP32 on large 3D grids: the same arithmetic as PolF32 under looser register
+// caps (tile.cuh, phase_min_blocks), chosen at launch by the grid's size.
+struct PolF32W : PolF32 {
+    static constexpr bool wide = true;
 };
 
 // Compensated BF16 storage (BP_PREC_CBF16): each value is the top 24 bits of
@@ -394,6 +402,7 @@ struct PolC16 {
     static constexpr int prec = BP_PREC_COMP16;
     static constexpr int store = BP_PREC_COMP16;
     static constexpr bool exact = false;
+    static constexpr bool wide = false;
     static constexpr bool graded = false;
     template <bool NC = false>
     __device__ __forceinline__ static void ld4(const void* p, const int8_t* lo, cidx i, real (&v)[4]) {

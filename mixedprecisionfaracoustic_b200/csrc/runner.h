@@ -7,6 +7,8 @@
 // an odd last step of a chunk by the tile kernels), the marching kernels
 // (step_march.cu) and the bulk-copy staged kernels (step_staged.cu).
 #pragma once
+#include <cstdlib>
+
 #include "shot.h"
 
 namespace bpk {
@@ -52,7 +54,9 @@ struct Runner {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        int ov = phase_occupancy(prec, dim, order, true, rounding), ot = phase_occupancy(prec, dim, order, false, rounding);
+        const bool wide = wide_grid();
+        int ov = phase_occupancy(prec, dim, order, true, rounding, wide),
+            ot = phase_occupancy(prec, dim, order, false, rounding, wide);
         if (ctas_per_sm > 0) { ov = ov < ctas_per_sm ? ov : ctas_per_sm; ot = ot < ctas_per_sm ? ot : ctas_per_sm; }
         long long gv = (long long)ov * sms, gt = (long long)ot * sms;
         grid_v = (int)(gv < tiles ? gv : (tiles > 0 ? tiles : 1));
@@ -114,13 +118,23 @@ struct Runner {
 #endif
         return post_in_t && !march && !staged;
     }
+    // large 3D FP32 launches take the looser register caps (PolF32W); the
+    // grid's occupancy follows the kernels that run
+    // (BP_WIDE_CELLS in the environment moves the threshold, for tests)
+    bool wide_grid() const {
+        static const long long thr = [] {
+            const char* e = std::getenv("BP_WIDE_CELLS");
+            return e ? std::atoll(e) : kWideCells;
+        }();
+        return dim == 3 && prec == BP_PREC_FP32 && rounding == BP_ROUND_FAST && !graded && ntiles * 1024 >= thr;
+    }
     // launches of one step of the two-phase kernels
     int launches_per_step() const { return fused_post() ? 2 : 3; }
     cudaError_t phase(bool v, int k) {
         if (march) return launch_phase_march(prec, order, v, d_shots, nshots, ntiles_m, k, st);
         if (staged) return launch_phase_staged(prec, order, v, d_shots, nshots, ntiles_s, k, grid_s, d_err, st);
         return launch_phase(prec, dim, order, v, d_shots, nshots, ntiles, k, v ? grid_v : grid_t, st,
-                            (!v && fused_post()) ? 1 : 0, rounding, multi_unit, graded);
+                            (!v && fused_post()) ? 1 : 0, rounding, multi_unit, graded, wide_grid());
     }
 
     // One step (index k of the chunk) of the two-phase kernels, or of the

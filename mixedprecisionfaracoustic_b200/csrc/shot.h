@@ -18,7 +18,9 @@ namespace bpk {
 // tile shape has more (row, segment) units than a CTA has warps
 cudaError_t launch_phase(int prec, int dim, int order, bool vphase, const ShotDesc* d_shots, int nshots,
                          long long ntiles, int k, int grid, cudaStream_t st, int post = 0, int rounding = 0,
-                         bool multi = false, bool graded = false);
+                         bool multi = false, bool graded = false, bool wide = false);
+// updated cells of a launch from which 3D FP32 takes the large-grid register caps (PolF32W)
+constexpr long long kWideCells = 16LL << 20;
 cudaError_t launch_post(int prec, const ShotDesc* d_shots, int nshots, int max_rec, int k, int do_record,
                         cudaStream_t st);
 cudaError_t launch_inject(int prec, const ShotDesc* d_shots, int nshots, int k, cudaStream_t st);
@@ -62,7 +64,7 @@ int staged_tile_rows();
 int staged_tile_width();
 cudaError_t launch_phase_staged(int prec, int order, bool vphase, const ShotDesc* d, int nshots, long long ntiles,
                                 int k, int grid, int* err, cudaStream_t st);
-int phase_occupancy(int prec, int dim, int order, bool vphase, int rounding = 0);
+int phase_occupancy(int prec, int dim, int order, bool vphase, int rounding = 0, bool wide = false);
 // register-window marching 2D phase kernels (step_march.cu)
 bool march_supported(int prec, int dim);
 bool march_default();            // whether BP_KERNEL_AUTO picks the marching kernels where supported

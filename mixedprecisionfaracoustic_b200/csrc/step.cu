@@ -209,6 +209,8 @@ struct Launch {
     }
         if constexpr (P::graded) {           // the variable z grid: order 2 only
             BPK_LAUNCH(2, 2) BPK_LAUNCH(3, 2)
+        } else if constexpr (P::wide) {      // large 3D grids only
+            BPK_LAUNCH(3, 2) BPK_LAUNCH(3, 4)
         } else {
             BPK_LAUNCH(2, 2) BPK_LAUNCH(2, 4) BPK_LAUNCH(3, 2) BPK_LAUNCH(3, 4)
         }
@@ -223,7 +225,9 @@ struct Launch {
 namespace bpk {
 cudaError_t launch_phase(int prec, int dim, int order, bool vphase, const ShotDesc* d_shots, int nshots,
                          long long ntiles, int k, int grid, cudaStream_t st, int post, int rounding, bool multi,
-                         bool graded) {
+                         bool graded, bool wide) {
+    if (wide && dim == 3 && prec == BP_PREC_FP32 && rounding == BP_ROUND_FAST && !graded)
+        return Launch<PolF32W>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
     if (graded) {
         if (prec != BP_PREC_FP32 || rounding != BP_ROUND_FAST || order != 2) return cudaErrorInvalidValue;
         return Launch<PolF32G>::phase(dim, order, vphase, d_shots, nshots, ntiles, k, grid, st, post, multi);
@@ -280,13 +284,15 @@ cudaError_t launch_field_f64(int prec, const ShotDesc* d_shots, int f, double* o
     return cudaGetLastError();
 }
 
-int phase_occupancy(int prec, int dim, int order, bool vphase, int rounding) {
+int phase_occupancy(int prec, int dim, int order, bool vphase, int rounding, bool wide) {
     int n = 0;
     const void* fn = nullptr;
 #define BPK_FN(PP, D, O)                                                                   \
     if (dim == D && order == O)                                                            \
         fn = vphase ? (const void*)k_phase<D, O, PP, true, false> : (const void*)k_phase<D, O, PP, false, false>;
-    if (prec == BP_PREC_FP32 && rounding == BP_ROUND_REFERENCE) {
+    if (wide && dim == 3 && prec == BP_PREC_FP32 && rounding == BP_ROUND_FAST) {
+        BPK_FN(PolF32W, 3, 2) BPK_FN(PolF32W, 3, 4)
+    } else if (prec == BP_PREC_FP32 && rounding == BP_ROUND_REFERENCE) {
         BPK_FN(PolF32R, 2, 2) BPK_FN(PolF32R, 2, 4) BPK_FN(PolF32R, 3, 2) BPK_FN(PolF32R, 3, 4)
     } else if (prec == BP_PREC_FP32) { BPK_FN(PolF32, 2, 2) BPK_FN(PolF32, 2, 4) BPK_FN(PolF32, 3, 2) BPK_FN(PolF32, 3, 4) }
     else if (prec == BP_PREC_COMP16) { BPK_FN(PolC16, 2, 2) BPK_FN(PolC16, 2, 4) BPK_FN(PolC16, 3, 2) BPK_FN(PolC16, 3, 4) }

@@ -64,15 +64,15 @@ __device__ __forceinline__ int locate_shot(const ShotDesc* shots, int nshots, lo
 #ifndef BP_MINB3_F32
 #define BP_MINB3_F32 3
 #endif
-// 3D FP32 at 2 CTAs (128 registers, no spills), measured on B200 (indexed
-// uniform media): the T phase 15 % faster at order 2 (300^3) and unchanged at
-// order 4 (200^3), the order-2 V phase 2 % faster; the order-4 V phase 12 %
-// slower, so it keeps 3
-#ifndef BP_MINB3_F32_T
-#define BP_MINB3_F32_T 2
-#endif
-#ifndef BP_MINB3_F32_V2
-#define BP_MINB3_F32_V2 2
+// 3D FP32 on large grids (PolF32W, from kWideCells updated cells of a launch):
+// 2 CTAs (128 registers, no spills) for the T phase and the order-2 V phase,
+// measured on B200: the 552 x 552 x 424 order-2 step 5 % faster (16,716 ->
+// 17,507 Mcell-updates/s) and the uniform 300^3 order-2 T phase 15 % faster,
+// while the 192^3 order-2 reference run (7 M cells) is 13 % slower (26 % with
+// reference rounding) and keeps 3; the order-4 V phase keeps 3 everywhere
+// (12 % slower at 2)
+#ifndef BP_MINB3_F32_WIDE
+#define BP_MINB3_F32_WIDE 2
 #endif
 #ifndef BP_MINB3_C16
 #define BP_MINB3_C16 4
@@ -94,8 +94,8 @@ __device__ __forceinline__ int locate_shot(const ShotDesc* shots, int nshots, lo
 template <int DIM, int ORD, class P, bool VPHASE>
 __host__ __device__ constexpr int phase_min_blocks() {
     if (P::store == BP_PREC_CBF16) return DIM == 3 ? BP_MINB3_B24 : (VPHASE ? BP_MINB_B24_V : BP_MINB_B24);
-    if (DIM == 3 && P::prec == BP_PREC_FP32) return VPHASE ? (ORD == 4 ? BP_MINB3_F32 : BP_MINB3_F32_V2) : BP_MINB3_F32_T;
-    if (DIM == 3) return P::prec == BP_PREC_COMP16 ? BP_MINB3_C16 : BP_MINB3_F64;
+    if (DIM == 3 && P::prec == BP_PREC_FP32 && P::wide) return (VPHASE && ORD == 4) ? BP_MINB3_F32 : BP_MINB3_F32_WIDE;
+    if (DIM == 3) return P::prec == BP_PREC_FP32 ? BP_MINB3_F32 : P::prec == BP_PREC_COMP16 ? BP_MINB3_C16 : BP_MINB3_F64;
     return P::prec == BP_PREC_FP32 ? BP_MINB_F32
                                    : P::prec == BP_PREC_COMP16 ? (VPHASE ? BP_MINB_C16_V : BP_MINB_C16) : BP_MINB_F64;
 }
